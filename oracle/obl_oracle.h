@@ -1,0 +1,117 @@
+/*
+ * obl_oracle.h -- FP64 CPU restatement of the OverlappingBLs hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py may load this library; the product path
+ * (libobl_b200.so) never links or calls it.
+ *
+ * Parity status: PARITY UNPINNED.  The reference (Fortran 90 + MPI + FFTW 3.3.x,
+ * the SBL/code Fortran sources) ships no tests, golden vectors or fixtures, and it cannot be
+ * compiled here (no Fortran compiler, no MPI, no FFTW).  This restatement is
+ * pinned instead against (1) analytic known-answer cases, (2) a long-double
+ * naive DFT, (3) an independent numpy restatement (tests/golden/gen_golden.py)
+ * and (4) the reference's own invariants (divergence-free projection, the
+ * pipelined multi-rank Thomas solve equal to the sequential one).
+ *
+ * Array conventions follow the reference exactly (Fortran column-major):
+ *   physical field  f(ldx, nyt, 0:nz)    -> f[x + ldx*(y + nyt*z)], x,y 0-based
+ *   spectral plane  c(lhx, nyt)          -> c[kx + lhx*ky]  (complex double)
+ *   padded plane    b(nxt2, nyt2)        -> b[x + nxt2*y]
+ *   dpdx/dpdy/dpdz  (ldx, nyt, 1:nz)     -> level jz stored at slot jz-1
+ * with ldx = 2*(nxt/2+1), nz = (nzt-1)/npz + 1 (SBL/code/102_initial.f90:119-141).
+ * The "global" arrays used here are the single-rank (npz = 1) arrays:
+ * nz = nzt, levels 0..nzt.
+ */
+#ifndef OBL_ORACLE_H
+#define OBL_ORACLE_H
+
+#include <complex.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_grid {
+    /* inputs (dimensional, as in the namelist &domain_param / &time_param) */
+    int nxt, nyt, nzt;
+    double lx_tot, ly_tot, lz_tot, z_i, dt, u_scale;
+    int ubc_stress_free;   /* project(): ubc_mom == 'stress free' (110_project.f90:51) */
+    /* derived by orc_grid_init (102_initial.f90:119-141, 186-199) */
+    int nz, lhx, lhy, ldx, ldy, nxt2, nyt2, lhx2, lhy2, ldx2, ldy2;
+    double lx, ly, lz, dz, dt_nd;   /* non-dimensional (divided by z_i; dt*u_scale/z_i) */
+} orc_grid;
+
+/* ---- FFT (own mixed-radix Cooley-Tukey; unnormalised, FFTW sign convention) ---- */
+/* sign = -1 forward (FFTW_FORWARD), +1 backward.  Any n >= 1. */
+void orc_fft_c2c(int n, const double complex *in, double complex *out, int sign);
+/* r2c: n reals -> n/2+1 complex.  c2r: n/2+1 complex -> n reals; ignores the
+   imaginary parts of the DC and (even n) Nyquist bins, as FFTW's c2r does. */
+void orc_fft_r2c(int n, const double *in, double complex *out);
+void orc_fft_c2r(int n, const double complex *in, double *out);
+/* naive O(n^2) DFT in long double, for validating the FFT */
+void orc_dft_naive(int n, const double complex *in, double complex *out, int sign);
+
+/* ---- setup ---- */
+int  orc_grid_init(orc_grid *g);    /* returns 0 on success, nonzero on a bad size */
+/* wavenumber tables of init_wavenumber (002_fft.f90:121-189), npy = 1:
+   kx[lhx], ky[lhy], kx2d/ky2d/k2[lhx*nyt], notnyq[lhx*nyt] (1 = not Nyquist) */
+void orc_wavenumbers(const orc_grid *g, double *kx, double *ky, double *kx2d,
+                     double *ky2d, double *k2, int *notnyq);
+
+/* ---- spectral derivatives (004_derivatives.f90) ----
+   nlev planes starting at level 0 of f(ldx, nyt, 0:nlev-1). Only x < nxt is written. */
+void orc_ddx(const orc_grid *g, double *dfdx, const double *fun, int nlev);
+void orc_ddy(const orc_grid *g, double *dfdy, const double *fun, int nlev);
+/* ddz_uv / ddz_w on the single-rank arrays (levels 0..nz), with the
+   coordz == 0 == npz-1 branches of 004_derivatives.f90:85-116,155-183 */
+void orc_ddz_uv(const orc_grid *g, double *dfdz, const double *fun);
+void orc_ddz_w(const orc_grid *g, double *dfdz, const double *fun);
+
+/* ---- 2D transforms of one plane (203_fftn_mpi.f90:4-67) ---- */
+void orc_fftn(const orc_grid *g, const double *in, double complex *out);
+void orc_ifftn(const orc_grid *g, const double complex *in, double *out);
+
+/* ---- 3/2-rule dealiasing of one plane (108_01_padd.f90:73-197) ---- */
+void orc_zero_padding(const orc_grid *g, const double *var, double *var_big);
+void orc_zero_unpadding(const orc_grid *g, const double *var_big, double *var);
+
+/* ---- Nyquist filter (006_test_filter.f90:82-105), nlev planes in place ---- */
+void orc_filter_data(const orc_grid *g, double *f, int nlev);
+
+/* ---- pressure solve (109_press_stag_array.f90) emulating npz z-ranks ----
+   npz = 1  : single-rank semantics (p_hat(nz-1) forced to 0: Dirichlet top).
+   npz >= 2 : pipelined multi-rank semantics (Neumann top row, divtz top plane used).
+   Inputs are the global single-rank arrays u,v,w(ldx,nyt,0:nzt); divtz_bot is the
+   plane divtz(:,:,1) of the bottom rank, divtz_top the plane divtz(:,:,nz) of the top
+   rank (global level nzt).  Outputs: p(ldx,nyt,0:nzt) levels 0..nzt-1 written,
+   dpdx/dpdy(ldx,nyt,1:nzt) levels 1..nzt-1 written.  Returns nonzero if
+   (nzt-1) % npz != 0. */
+int orc_press_stag_array(const orc_grid *g, int npz, const double *u,
+                         const double *v, const double *w,
+                         const double *divtz_bot, const double *divtz_top,
+                         double *p, double *dpdx, double *dpdy);
+
+/* flosol glue (103_flosol.f90:169-175): dpdz(jz) = (p(jz)-p(jz-1))/dz, jz=1..nz-1 */
+void orc_dpdz(const orc_grid *g, const double *p, double *dpdz);
+
+/* project() (110_project.f90:4-62) on the global arrays (bottom and top rank at once) */
+void orc_project(const orc_grid *g, double *u, double *v, double *w,
+                 const double *dpdx, const double *dpdy, const double *dpdz);
+
+/* Headline step: ddx/ddy and zero_padding of u,v,w,theta on levels 0..nz, then
+   press_stag_array(u,v,w) (divtz = 0), dpdz and project().  d[8] = dudx,dudy,dvdx,
+   dvdy,dwdx,dwdy,dtdx,dtdy (ldx,nyt,0:nz); big[4] = u,v,w,theta padded
+   (nxt2,nyt2,0:nz); p (ldx,nyt,0:nz); dp[3] = dpdx,dpdy,dpdz (ldx,nyt,1:nz);
+   u,v,w updated in place. */
+int orc_step(const orc_grid *g, int npz, double *u, double *v, double *w,
+             const double *theta, double *const d[8], double *const big[4],
+             double *p, double *const dp[3]);
+
+/* threads used by the OpenMP loops (0 = leave the OpenMP default) */
+void orc_set_threads(int n);
+int  orc_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
