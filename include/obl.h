@@ -1,0 +1,181 @@
+/*
+ * obl.h -- C ABI of the B200-native OverlappingBLs hot path (libobl_b200.so).
+ *
+ * This is the drop-in boundary for the reference's derivative and pressure-solver
+ * routines.  Each entry point names the Fortran routine it replaces (paths relative
+ * to the reference project; SBL/code is canonical, BBL/SBBL carry identical copies).
+ * A Fortran caller binds these through ISO_C_BINDING (overlappingbls_b200/fortran/
+ * obl_gpu.f90) and keeps the reference call signatures.
+ *
+ * Conventions
+ *   - Every function returns an int status (OBL_OK = 0); obl_last_error() gives text.
+ *   - Arrays use the reference's Fortran layout (column-major, x fastest):
+ *       physical field   f(ldx, nyt, 0:nz)        ldx = 2*(nxt/2+1), nz = nzt
+ *       level-1-based    dpdx/dpdy/dpdz(ldx, nyt, 1:nz)   (slot jz-1 holds level jz)
+ *       padded field     b(nxt2, nyt2, 0:nz)      nxt2 = 3*nxt/2
+ *       spectral plane   c(lhx, nyt) complex      lhx = nxt/2+1 (interleaved re,im)
+ *     One GPU holds the whole domain (npy = 1 and the z-slabs of all ranks).
+ *   - Host variants take double* host arrays (Fortran real(8)); the library stages
+ *     them through device buffers it owns.  Only the elements the reference routine
+ *     writes are written back (e.g. x < nxt of each row), so pad columns and levels
+ *     the reference leaves alone keep their host values.
+ *   - *_dev variants take device pointers in the context's storage type: double for
+ *     OBL_PREC_F64, float for OBL_PREC_MIXED / OBL_PREC_F32.  They are asynchronous
+ *     on the context's stream.
+ *   - A context is bound to one device and one stream and is not reentrant: use one
+ *     context per host thread (the reference is single-threaded per MPI rank).
+ */
+#ifndef OBL_H
+#define OBL_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define OBL_OK 0
+#define OBL_ERR_ARG 1         /* bad argument or shape                         */
+#define OBL_ERR_CUDA 2        /* CUDA runtime error                            */
+#define OBL_ERR_NOMEM 3       /* device or pinned-host allocation failed       */
+#define OBL_ERR_TIMEOUT 4     /* a bounded device-side wait expired            */
+#define OBL_ERR_UNSUPPORTED 5 /* grid size without a compiled FFT plan         */
+#define OBL_ERR_NODEV 6       /* no CUDA device                                */
+
+/* ---- precision modes ---- */
+#define OBL_PREC_F64 0   /* every kernel in FP64 (the plain FP64 GPU form)             */
+#define OBL_PREC_MIXED 1 /* FP32 FFTs/dealiasing/TDMA, FP64 TDMA for (0,0) and low |k| */
+#define OBL_PREC_F32 2   /* FP32 everywhere (diagnostic)                                */
+
+/* ---- top boundary of the pressure solve (109_press_stag_array.f90:20-50,280-297) ---- */
+#define OBL_TOP_SINGLE_RANK 0 /* npz = 1 semantics: p_hat(nz-1) forced to 0 (Dirichlet) */
+#define OBL_TOP_NEUMANN 1     /* npz >= 2 semantics: Neumann top row, divtz top plane   */
+
+typedef struct obl_ctx obl_ctx;
+
+/* Grid and run constants, dimensional as in the namelist (&domain_param, &time_param,
+   &flow_param); non-dimensionalised exactly as init_parameter/init_nondimensional do
+   (102_initial.f90:119-141,186-199). */
+typedef struct obl_grid {
+    int nxt, nyt, nzt;
+    double lx_tot, ly_tot, lz_tot, z_i, dt, u_scale;
+} obl_grid;
+
+typedef struct obl_options {
+    int precision;        /* OBL_PREC_*                                          */
+    int top_bc;           /* OBL_TOP_*                                           */
+    int ubc_stress_free;  /* project(): ubc_mom == 'stress free' (110_project.f90:51) */
+    double fp64_k2_max;   /* MIXED: columns with k^2 <= this are solved in FP64;
+                             a negative value selects the built-in default       */
+    int device;           /* CUDA device ordinal                                  */
+} obl_options;
+
+typedef struct obl_info {
+    int nxt, nyt, nzt, nz, ldx, lhx, nxt2, nyt2;
+    int elem_bytes;              /* storage bytes per real (8 or 4)               */
+    int n_fp64_columns;          /* MIXED: (kx,ky) columns solved in FP64         */
+    double dz, dt_nd, lx, ly;    /* non-dimensional                               */
+    long long field_elems;       /* ldx*nyt*(nz+1)                                */
+    long long dfield_elems;      /* ldx*nyt*nz                                    */
+    long long big_elems;         /* nxt2*nyt2*(nz+1)                              */
+    long long spec_elems;        /* lhx*nyt complex per plane                     */
+} obl_info;
+
+/* ---- context: replaces init_parameter, init_fft_plan, init_wavenumber and
+        init_coef_press + tdmaMcoef_pipelined (102_initial.f90:20-53,
+        002_fft.f90:78-189, 109_press_stag_array.f90:4-103) ---- */
+int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out);
+int obl_ctx_destroy(obl_ctx *ctx);
+int obl_ctx_info(const obl_ctx *ctx, obl_info *info);
+int obl_set_stream(obl_ctx *ctx, void *cuda_stream);  /* cudaStream_t; NULL = legacy */
+int obl_synchronize(obl_ctx *ctx);
+int obl_last_error(const obl_ctx *ctx, char *buf, size_t n);
+/* kernels launched by this context so far */
+long long obl_launch_count(const obl_ctx *ctx);
+/* per-kernel CUDA-event timing: enable, then read a JSON object
+   {"kernel": [launches, total_ms], ...} (synchronizes; clears the records) */
+int obl_timing_enable(obl_ctx *ctx, int on);
+int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
+
+/* ---- spectral derivatives: ddx / ddy (004_derivatives.f90:18-41, 45-81) ----
+   fields (ldx, nyt, nlev) (the reference passes nlev = nz+1); x < nxt written. */
+int obl_ddx(obl_ctx *ctx, double *dfdx, const double *fun, int nlev);
+int obl_ddy(obl_ctx *ctx, double *dfdy, const double *fun, int nlev);
+int obl_ddx_dev(obl_ctx *ctx, void *dfdx, const void *fun, int nlev);
+int obl_ddy_dev(obl_ctx *ctx, void *dfdy, const void *fun, int nlev);
+
+/* ---- vertical differences: ddz_uv / ddz_w (004_derivatives.f90:85-116, 155-183) ----
+   single-rank branches: ddz_uv writes levels 0 (BOGUS) and 2..nz-1;
+   ddz_w writes levels 0 (BOGUS), 1..nz-1 and nz (= 0). */
+int obl_ddz_uv(obl_ctx *ctx, double *dfdz, const double *fun);
+int obl_ddz_w(obl_ctx *ctx, double *dfdz, const double *fun);
+int obl_ddz_uv_dev(obl_ctx *ctx, void *dfdz, const void *fun);
+int obl_ddz_w_dev(obl_ctx *ctx, void *dfdz, const void *fun);
+
+/* ---- 2D transforms fftn_mpi / ifftn_mpi (203_fftn_mpi.f90:4-35, 39-67) ----
+   in (ldx, nyt, nlev) real -> out (lhx, nyt, nlev) complex, unnormalised, x- and
+   y-Nyquist zeroed; ifftn: complex -> real, x < nxt written. */
+int obl_fftn(obl_ctx *ctx, const double *in, double *out_cplx, int nlev);
+int obl_ifftn(obl_ctx *ctx, const double *in_cplx, double *out, int nlev);
+int obl_fftn_dev(obl_ctx *ctx, const void *in, void *out_cplx, int nlev);
+int obl_ifftn_dev(obl_ctx *ctx, const void *in_cplx, void *out, int nlev);
+
+/* ---- 3/2-rule dealiasing zero_padding / zero_unpadding (108_01_padd.f90:73-197) ----
+   var (ldx, nyt, nlev) <-> var_big (nxt2, nyt2, nlev). */
+int obl_zero_padding(obl_ctx *ctx, const double *var, double *var_big, int nlev);
+int obl_zero_unpadding(obl_ctx *ctx, const double *var_big, double *var, int nlev);
+int obl_zero_padding_dev(obl_ctx *ctx, const void *var, void *var_big, int nlev);
+int obl_zero_unpadding_dev(obl_ctx *ctx, const void *var_big, void *var, int nlev);
+
+/* ---- filter_data (006_test_filter.f90:82-105): in place on (ldx, nyt, nlev) ---- */
+int obl_filter_data(obl_ctx *ctx, double *f, int nlev);
+int obl_filter_data_dev(obl_ctx *ctx, void *f, int nlev);
+
+/* ---- press_stag_array + tdmaSolver_pipelined (109_press_stag_array.f90:107-319) ----
+   u,v,w (ldx,nyt,0:nz) in; divtz_bot = divtz(:,:,1), divtz_top = divtz(:,:,nz)
+   planes (ldx,nyt) or NULL for zero (the theta/lbc==0 surface term of :187-192 is
+   folded into divtz_bot by the caller); p (ldx,nyt,0:nz) levels 0..nz-1 written;
+   dpdx, dpdy (ldx,nyt,1:nz) levels 1..nz-1 written. */
+int obl_press_stag_array(obl_ctx *ctx, const double *u, const double *v, const double *w,
+                         const double *divtz_bot, const double *divtz_top,
+                         double *p, double *dpdx, double *dpdy);
+int obl_press_stag_array_dev(obl_ctx *ctx, const void *u, const void *v, const void *w,
+                             const void *divtz_bot, const void *divtz_top,
+                             void *p, void *dpdx, void *dpdy);
+
+/* ---- flosol glue (103_flosol.f90:174-175): dpdz(jz)=(p(jz)-p(jz-1))/dz, 1..nz-1 ---- */
+int obl_dpdz(obl_ctx *ctx, const double *p, double *dpdz);
+int obl_dpdz_dev(obl_ctx *ctx, const void *p, void *dpdz);
+
+/* ---- project (110_project.f90:4-62): u,v,w updated in place ---- */
+int obl_project(obl_ctx *ctx, double *u, double *v, double *w,
+                const double *dpdx, const double *dpdy, const double *dpdz);
+int obl_project_dev(obl_ctx *ctx, void *u, void *v, void *w,
+                    const void *dpdx, const void *dpdy, const void *dpdz);
+
+/* ---- fused projection-plus-derivative step ----
+   The hot-path slice of one flosol time step on u,v,w,theta: ddx/ddy of
+   u,v,w,theta and zero_padding of u,v,w,theta on levels 0..nz (103_flosol.f90:30-35,
+   108_convec.f90:38-42, 010_scalars.f90:137-138,429-431), press_stag_array(u,v,w),
+   dpdz and project (103_flosol.f90:168-188).  Pointers are host (obl_step /
+   obl_step_f32) or device (obl_step_dev, storage type). */
+typedef struct obl_step_io {
+    void *u, *v, *w;          /* in/out (ldx,nyt,0:nz), projected in place         */
+    const void *theta;        /* in (ldx,nyt,0:nz)                                  */
+    void *d[8];               /* out dudx,dudy,dvdx,dvdy,dwdx,dwdy,dtdx,dtdy         */
+    void *big[4];             /* out u,v,w,theta on the 3/2 grid (nxt2,nyt2,0:nz)    */
+    void *p;                  /* out (ldx,nyt,0:nz)                                 */
+    void *dp[3];              /* out dpdx,dpdy,dpdz (ldx,nyt,1:nz)                  */
+    const void *divtz_bot;    /* optional plane (ldx,nyt), NULL = 0                 */
+    const void *divtz_top;    /* optional plane (ldx,nyt), NULL = 0                 */
+} obl_step_io;
+
+int obl_step(obl_ctx *ctx, const obl_step_io *io);      /* host double*   */
+int obl_step_f32(obl_ctx *ctx, const obl_step_io *io);  /* host float*    */
+int obl_step_dev(obl_ctx *ctx, const obl_step_io *io);  /* device, storage type */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,330 @@
+"""OverlappingBLs hot path on B200: Python binding of the C ABI (include/obl.h).
+
+The product is libobl_b200.so (hand-written sm_100a CUDA kernels behind a C ABI).
+This module loads it with ctypes and mirrors the reference's Fortran routine names
+and argument order (output first, input second, as in ``call ddx(dfdx, fun)``,
+SBL/code/004_derivatives.f90:18).  There is no CPU fallback: if the library is
+missing or no GPU is present, constructing a Context raises.
+
+Host arrays are numpy arrays in the reference's Fortran layout (``order='F'``):
+    physical field  (ldx, nyt, nz+1)  float64     ldx = 2*(nxt/2+1), nz = nzt
+    dpdx/dpdy/dpdz  (ldx, nyt, nz)    float64     (slot jz-1 holds level jz)
+    padded field    (nxt2, nyt2, nlev)
+    spectral        (lhx, nyt, nlev)  complex128
+``*_dev`` methods take integer device pointers in the context's storage type
+(float64 for precision="f64", float32 for "mixed"/"f32").
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libobl_b200.so")
+
+OBL_OK = 0
+ERRORS = {1: "OBL_ERR_ARG", 2: "OBL_ERR_CUDA", 3: "OBL_ERR_NOMEM", 4: "OBL_ERR_TIMEOUT",
+          5: "OBL_ERR_UNSUPPORTED", 6: "OBL_ERR_NODEV"}
+PRECISION = {"f64": 0, "mixed": 1, "f32": 2}
+TOP_BC = {"single": 0, "neumann": 1}
+
+# every symbol declared in include/obl.h
+EXPORTS = [
+    "obl_ctx_create", "obl_ctx_destroy", "obl_ctx_info", "obl_set_stream", "obl_synchronize",
+    "obl_last_error", "obl_launch_count", "obl_timing_enable", "obl_timing_report",
+    "obl_ddx", "obl_ddy", "obl_ddx_dev", "obl_ddy_dev",
+    "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
+    "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
+    "obl_zero_padding", "obl_zero_unpadding", "obl_zero_padding_dev", "obl_zero_unpadding_dev",
+    "obl_filter_data", "obl_filter_data_dev",
+    "obl_press_stag_array", "obl_press_stag_array_dev",
+    "obl_dpdz", "obl_dpdz_dev", "obl_project", "obl_project_dev",
+    "obl_step", "obl_step_f32", "obl_step_dev",
+]
+
+
+class OblError(RuntimeError):
+    pass
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nxt", ctypes.c_int), ("nyt", ctypes.c_int), ("nzt", ctypes.c_int),
+                ("lx_tot", ctypes.c_double), ("ly_tot", ctypes.c_double),
+                ("lz_tot", ctypes.c_double), ("z_i", ctypes.c_double),
+                ("dt", ctypes.c_double), ("u_scale", ctypes.c_double)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("top_bc", ctypes.c_int),
+                ("ubc_stress_free", ctypes.c_int), ("fp64_k2_max", ctypes.c_double),
+                ("device", ctypes.c_int)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("nxt", ctypes.c_int), ("nyt", ctypes.c_int), ("nzt", ctypes.c_int),
+                ("nz", ctypes.c_int), ("ldx", ctypes.c_int), ("lhx", ctypes.c_int),
+                ("nxt2", ctypes.c_int), ("nyt2", ctypes.c_int), ("elem_bytes", ctypes.c_int),
+                ("n_fp64_columns", ctypes.c_int), ("dz", ctypes.c_double),
+                ("dt_nd", ctypes.c_double), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+                ("field_elems", ctypes.c_longlong), ("dfield_elems", ctypes.c_longlong),
+                ("big_elems", ctypes.c_longlong), ("spec_elems", ctypes.c_longlong)]
+
+
+class StepIO(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p),
+                ("theta", ctypes.c_void_p), ("d", ctypes.c_void_p * 8),
+                ("big", ctypes.c_void_p * 4), ("p", ctypes.c_void_p),
+                ("dp", ctypes.c_void_p * 3), ("divtz_bot", ctypes.c_void_p),
+                ("divtz_top", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libobl_b200.so; raises OblError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OblError(f"{path} is missing: build it with `python -m overlappingbls_b200.build`")
+    L = ctypes.CDLL(path)
+    P, I, C = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char)
+    ctx = ctypes.c_void_p
+    sig = {
+        "obl_ctx_create": [ctypes.POINTER(Grid), ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)],
+        "obl_ctx_destroy": [ctx], "obl_ctx_info": [ctx, ctypes.POINTER(Info)],
+        "obl_set_stream": [ctx, P], "obl_synchronize": [ctx],
+        "obl_last_error": [ctx, ctypes.c_char_p, ctypes.c_size_t],
+        "obl_timing_enable": [ctx, I], "obl_timing_report": [ctx, ctypes.c_char_p, ctypes.c_size_t],
+        "obl_ddx": [ctx, P, P, I], "obl_ddy": [ctx, P, P, I],
+        "obl_ddx_dev": [ctx, P, P, I], "obl_ddy_dev": [ctx, P, P, I],
+        "obl_ddz_uv": [ctx, P, P], "obl_ddz_w": [ctx, P, P],
+        "obl_ddz_uv_dev": [ctx, P, P], "obl_ddz_w_dev": [ctx, P, P],
+        "obl_fftn": [ctx, P, P, I], "obl_ifftn": [ctx, P, P, I],
+        "obl_fftn_dev": [ctx, P, P, I], "obl_ifftn_dev": [ctx, P, P, I],
+        "obl_zero_padding": [ctx, P, P, I], "obl_zero_unpadding": [ctx, P, P, I],
+        "obl_zero_padding_dev": [ctx, P, P, I], "obl_zero_unpadding_dev": [ctx, P, P, I],
+        "obl_filter_data": [ctx, P, I], "obl_filter_data_dev": [ctx, P, I],
+        "obl_press_stag_array": [ctx, P, P, P, P, P, P, P, P],
+        "obl_press_stag_array_dev": [ctx, P, P, P, P, P, P, P, P],
+        "obl_dpdz": [ctx, P, P], "obl_dpdz_dev": [ctx, P, P],
+        "obl_project": [ctx, P, P, P, P, P, P], "obl_project_dev": [ctx, P, P, P, P, P, P],
+        "obl_step": [ctx, ctypes.POINTER(StepIO)], "obl_step_f32": [ctx, ctypes.POINTER(StepIO)],
+        "obl_step_dev": [ctx, ctypes.POINTER(StepIO)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = I
+    L.obl_launch_count.argtypes = [ctx]
+    L.obl_launch_count.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+def _ptr(a, dtype=np.float64):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if not isinstance(a, np.ndarray):
+        raise TypeError("expected a numpy array or an integer device pointer")
+    if a.dtype != dtype:
+        raise TypeError(f"expected dtype {np.dtype(dtype)}, got {a.dtype}")
+    if not (a.flags["F_CONTIGUOUS"] or a.ndim <= 1):
+        raise TypeError("host arrays must be Fortran-ordered (order='F')")
+    return a.ctypes.data
+
+
+class Context:
+    """One grid on one GPU: replaces init_parameter / init_fft_plan / init_coef_press."""
+
+    def __init__(self, nxt, nyt, nzt, lx_tot, ly_tot, lz_tot, z_i, dt, u_scale=1.0,
+                 precision="f64", top_bc="neumann", ubc_stress_free=False, fp64_k2_max=-1.0,
+                 device=0):
+        self._lib = load_library()
+        g = Grid(nxt, nyt, nzt, lx_tot, ly_tot, lz_tot, z_i, dt, u_scale)
+        o = Options(PRECISION[precision], TOP_BC[top_bc], 1 if ubc_stress_free else 0,
+                    float(fp64_k2_max), int(device))
+        h = ctypes.c_void_p()
+        rc = self._lib.obl_ctx_create(ctypes.byref(g), ctypes.byref(o), ctypes.byref(h))
+        if rc != OBL_OK:
+            raise OblError(f"obl_ctx_create failed: {ERRORS.get(rc, rc)}")
+        self._h = h
+        self.precision = precision
+        self.top_bc = top_bc
+        inf = Info()
+        self._lib.obl_ctx_info(self._h, ctypes.byref(inf))
+        self.info = {k: getattr(inf, k) for k, _ in Info._fields_}
+        for k in ("nxt", "nyt", "nzt", "nz", "ldx", "lhx", "nxt2", "nyt2", "dz", "dt_nd"):
+            setattr(self, k, self.info[k])
+        self.dtype = np.float64 if self.info["elem_bytes"] == 8 else np.float32
+
+    # ---- lifecycle / plumbing ----
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.obl_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != OBL_OK:
+            buf = ctypes.create_string_buffer(1024)
+            self._lib.obl_last_error(self._h, buf, 1024)
+            raise OblError(f"{what}: {ERRORS.get(rc, rc)} {buf.value.decode()}")
+
+    def set_stream(self, stream_handle):
+        self._check(self._lib.obl_set_stream(self._h, stream_handle), "obl_set_stream")
+
+    def synchronize(self):
+        self._check(self._lib.obl_synchronize(self._h), "obl_synchronize")
+
+    def launch_count(self):
+        return int(self._lib.obl_launch_count(self._h))
+
+    def timing(self, on=True):
+        self._check(self._lib.obl_timing_enable(self._h, 1 if on else 0), "obl_timing_enable")
+
+    def timing_report(self):
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.obl_timing_report(self._h, buf, 1 << 16), "obl_timing_report")
+        return json.loads(buf.value.decode())
+
+    # ---- array helpers (Fortran layout) ----
+    def field(self, nlev=None, dtype=np.float64):
+        return np.zeros((self.ldx, self.nyt, self.nz + 1 if nlev is None else nlev), dtype, order="F")
+
+    def dfield(self, dtype=np.float64):
+        return np.zeros((self.ldx, self.nyt, self.nz), dtype, order="F")
+
+    def big_field(self, nlev=None, dtype=np.float64):
+        return np.zeros((self.nxt2, self.nyt2, self.nz + 1 if nlev is None else nlev), dtype, order="F")
+
+    def spectral(self, nlev=None):
+        return np.zeros((self.lhx, self.nyt, self.nz + 1 if nlev is None else nlev), np.complex128,
+                        order="F")
+
+    @staticmethod
+    def _nlev(a):
+        return a.shape[2] if a.ndim == 3 else 1
+
+    # ---- reference routines, host arrays (output first, as in the Fortran) ----
+    def ddx(self, dfdx, fun):
+        self._check(self._lib.obl_ddx(self._h, _ptr(dfdx), _ptr(fun), self._nlev(fun)), "ddx")
+
+    def ddy(self, dfdy, fun):
+        self._check(self._lib.obl_ddy(self._h, _ptr(dfdy), _ptr(fun), self._nlev(fun)), "ddy")
+
+    def ddz_uv(self, dfdz, fun):
+        self._check(self._lib.obl_ddz_uv(self._h, _ptr(dfdz), _ptr(fun)), "ddz_uv")
+
+    def ddz_w(self, dfdz, fun):
+        self._check(self._lib.obl_ddz_w(self._h, _ptr(dfdz), _ptr(fun)), "ddz_w")
+
+    def fftn(self, fin, fout):
+        self._check(self._lib.obl_fftn(self._h, _ptr(fin), _ptr(fout, np.complex128),
+                                       self._nlev(fin)), "fftn")
+
+    def ifftn(self, fin, fout):
+        self._check(self._lib.obl_ifftn(self._h, _ptr(fin, np.complex128), _ptr(fout),
+                                        self._nlev(fout)), "ifftn")
+
+    def zero_padding(self, var, var_big):
+        self._check(self._lib.obl_zero_padding(self._h, _ptr(var), _ptr(var_big),
+                                               self._nlev(var)), "zero_padding")
+
+    def zero_unpadding(self, var_big, var):
+        self._check(self._lib.obl_zero_unpadding(self._h, _ptr(var_big), _ptr(var),
+                                                 self._nlev(var_big)), "zero_unpadding")
+
+    def filter_data(self, f):
+        self._check(self._lib.obl_filter_data(self._h, _ptr(f), self._nlev(f)), "filter_data")
+
+    def press_stag_array(self, func, dfdx, dfdy, u, v, w, divtz_bot=None, divtz_top=None):
+        self._check(self._lib.obl_press_stag_array(
+            self._h, _ptr(u), _ptr(v), _ptr(w), _ptr(divtz_bot), _ptr(divtz_top),
+            _ptr(func), _ptr(dfdx), _ptr(dfdy)), "press_stag_array")
+
+    def dpdz(self, dpdz, p):
+        self._check(self._lib.obl_dpdz(self._h, _ptr(p), _ptr(dpdz)), "dpdz")
+
+    def project(self, u, v, w, dpdx, dpdy, dpdz):
+        self._check(self._lib.obl_project(self._h, _ptr(u), _ptr(v), _ptr(w), _ptr(dpdx),
+                                          _ptr(dpdy), _ptr(dpdz)), "project")
+
+    def _stepio(self, u, v, w, theta, d, big, p, dp, divtz_bot=None, divtz_top=None, dtype=np.float64):
+        io = StepIO()
+        pp = lambda a: _ptr(a, dtype)
+        io.u, io.v, io.w, io.theta, io.p = pp(u), pp(v), pp(w), pp(theta), pp(p)
+        for i in range(8):
+            io.d[i] = pp(d[i])
+        for i in range(4):
+            io.big[i] = pp(big[i])
+        for i in range(3):
+            io.dp[i] = pp(dp[i])
+        io.divtz_bot, io.divtz_top = pp(divtz_bot), pp(divtz_top)
+        return io
+
+    def step(self, u, v, w, theta, d, big, p, dp, divtz_bot=None, divtz_top=None):
+        """Fused step with host arrays (float64, or float32 through obl_step_f32)."""
+        dt = u.dtype.type if isinstance(u, np.ndarray) else np.float64
+        io = self._stepio(u, v, w, theta, d, big, p, dp, divtz_bot, divtz_top, dt)
+        fn = self._lib.obl_step_f32 if dt == np.float32 else self._lib.obl_step
+        self._check(fn(self._h, ctypes.byref(io)), "step")
+
+    # ---- device-pointer variants (integers; storage type) ----
+    def ddx_dev(self, dfdx, fun, nlev):
+        self._check(self._lib.obl_ddx_dev(self._h, dfdx, fun, nlev), "ddx_dev")
+
+    def ddy_dev(self, dfdy, fun, nlev):
+        self._check(self._lib.obl_ddy_dev(self._h, dfdy, fun, nlev), "ddy_dev")
+
+    def zero_padding_dev(self, var, var_big, nlev):
+        self._check(self._lib.obl_zero_padding_dev(self._h, var, var_big, nlev), "zero_padding_dev")
+
+    def zero_unpadding_dev(self, var_big, var, nlev):
+        self._check(self._lib.obl_zero_unpadding_dev(self._h, var_big, var, nlev), "zero_unpadding_dev")
+
+    def fftn_dev(self, fin, fout, nlev):
+        self._check(self._lib.obl_fftn_dev(self._h, fin, fout, nlev), "fftn_dev")
+
+    def ifftn_dev(self, fin, fout, nlev):
+        self._check(self._lib.obl_ifftn_dev(self._h, fin, fout, nlev), "ifftn_dev")
+
+    def filter_data_dev(self, f, nlev):
+        self._check(self._lib.obl_filter_data_dev(self._h, f, nlev), "filter_data_dev")
+
+    def press_stag_array_dev(self, func, dfdx, dfdy, u, v, w, divtz_bot=None, divtz_top=None):
+        self._check(self._lib.obl_press_stag_array_dev(self._h, u, v, w, divtz_bot, divtz_top,
+                                                       func, dfdx, dfdy), "press_stag_array_dev")
+
+    def dpdz_dev(self, dpdz, p):
+        self._check(self._lib.obl_dpdz_dev(self._h, p, dpdz), "dpdz_dev")
+
+    def project_dev(self, u, v, w, dpdx, dpdy, dpdz):
+        self._check(self._lib.obl_project_dev(self._h, u, v, w, dpdx, dpdy, dpdz), "project_dev")
+
+    def step_dev(self, u, v, w, theta, d, big, p, dp, divtz_bot=None, divtz_top=None):
+        io = StepIO()
+        io.u, io.v, io.w, io.theta, io.p = u, v, w, theta, p
+        for i in range(8):
+            io.d[i] = d[i]
+        for i in range(4):
+            io.big[i] = big[i]
+        for i in range(3):
+            io.dp[i] = dp[i]
+        io.divtz_bot, io.divtz_top = divtz_bot, divtz_top
+        self._check(self._lib.obl_step_dev(self._h, ctypes.byref(io)), "step_dev")

@@ -1,0 +1,924 @@
+// api.cu -- the C ABI of include/obl.h: context setup and every hot-path entry point.
+//
+// One context = one device, one stream, one grid.  It replaces the reference's
+// init_parameter / init_fft_plan / init_wavenumber / init_coef_press (tables are built
+// once: twiddles w_N^m in the storage precision, kx/ky wavenumbers in FP64, the FP64
+// island list of the mixed mode) and owns the device work buffers.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "lines.cuh"
+#include "press.cuh"
+
+using namespace obl;
+
+namespace {
+constexpr double kPi = 3.1415926535897932384626433;   // 001_param.f90:32
+constexpr double kTadv1 = 1.5;                         // 001_param.f90:152
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+};
+} // namespace
+
+struct obl_ctx {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    obl_grid grid{};
+    obl_options opt{};
+    int nxt = 0, nyt = 0, nzt = 0, nz = 0, L = 0, lhx = 0, lhy = 0, ldx = 0, nxt2 = 0, nyt2 = 0;
+    double lx = 0, ly = 0, dz = 0, dt_nd = 0;
+    std::string err;
+    Recorder rec;
+    bool f64 = true;
+    // tables
+    double *d_kx = nullptr;    // kx(lhx), Nyquist 0
+    double *d_ky1 = nullptr;   // ky(lhy), Nyquist 0 (1D, for ddy)
+    double *d_ky2 = nullptr;   // ky_2d row (nyt), Nyquist row 0
+    std::map<int, void *> tw;  // length -> w_N^m table in the storage precision
+    // FP64 islands (mixed mode)
+    int n_isl = 0;
+    int *d_isl = nullptr;
+    unsigned char *d_skip = nullptr;
+    // work buffers
+    DevBuf spec[4];            // Hx, Hy, Hz, phat (lhx*nyt*(nz+1) complex)
+    DevBuf cscr;               // c' scratch
+    DevBuf isl_c, isl_d;
+    DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
+    std::vector<DevBuf> stage; // host-variant staging (storage type)
+    std::vector<DevBuf> stage64;
+
+    size_t es() const { return f64 ? 8 : 4; }
+    long long plane() const { return (long long)ldx * nyt; }
+    long long field() const { return plane() * (nz + 1); }
+    long long dfield() const { return plane() * nz; }
+    long long sp() const { return (long long)lhx * nyt; }
+    long long big() const { return (long long)nxt2 * nyt2 * (nz + 1); }
+};
+
+// ----------------------------------------------------------------------------- helpers
+static int fail(obl_ctx *c, int code, const std::string &m)
+{
+    if (c) c->err = m;
+    return code;
+}
+static int cuda_fail(obl_ctx *c, cudaError_t e, const char *where)
+{
+    return fail(c, OBL_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);                                   \
+    } while (0)
+#define CTX_OK()                                                                                   \
+    do {                                                                                           \
+        if (!ctx) return OBL_ERR_ARG;                                                              \
+        cudaError_t e_ = cudaSetDevice(ctx->dev);                                                  \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, "cudaSetDevice");                         \
+    } while (0)
+
+static int ensure(obl_ctx *ctx, DevBuf &b, size_t bytes)
+{
+    if (b.n >= bytes) return OBL_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.n = 0;
+    if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, OBL_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    b.n = bytes;
+    return OBL_OK;
+}
+
+template <typename T> static const C2<T> *twt(obl_ctx *c, int n) { return (const C2<T> *)c->tw.at(n); }
+
+static bool len_ok(int n)
+{
+    switch (n) {
+    case 32: case 48: case 64: case 96: case 128: case 192: case 256: case 384: case 512: return true;
+    }
+    return false;
+}
+
+// ----------------------------------------------------------------------------- typed ops
+namespace {
+
+template <typename T> struct Ops {
+    obl_ctx *ctx;
+    cudaStream_t s() const { return ctx->stream; }
+
+    int chk(cudaError_t e, const char *w) { return e == cudaSuccess ? OBL_OK : cuda_fail(ctx, e, w); }
+
+    int rows(int op, int n, const RowArgs<T> &a, const char *name)
+    {
+        LaunchScope ls(ctx->rec, name, s());
+        return chk(launch_rows<T>(op, n, a, s()), name);
+    }
+    int cols(int op, bool real, int n, const ColArgs<T> &a, const char *name)
+    {
+        LaunchScope ls(ctx->rec, name, s());
+        return chk(launch_cols<T>(op, real, n, a, s()), name);
+    }
+
+    RowArgs<T> rowargs(const void *src, long long ss, void *dst, long long ds, long long nrows, double scale,
+                       int nin, int nout)
+    {
+        RowArgs<T> a{};
+        a.src = src; a.dst = dst; a.src_stride = ss; a.dst_stride = ds; a.npairs = nrows / 2;
+        a.scale = (T)scale; a.ktab = ctx->d_kx; a.twI = twt<T>(ctx, nin); a.twO = twt<T>(ctx, nout);
+        a.pad_scale = (T)1; a.pad_mode = 0;
+        return a;
+    }
+    ColArgs<T> colargs(const void *src, long long srow, long long spl, void *dst, long long drow, long long dpl,
+                       int ncols, int nlev, double scale, int nin, int nout)
+    {
+        ColArgs<T> a{};
+        a.src = src; a.dst = dst; a.src_row = srow; a.dst_row = drow; a.src_plane = spl; a.dst_plane = dpl;
+        a.ncols = ncols; a.nlev = nlev; a.scale = (T)scale; a.ktab = ctx->d_ky1;
+        a.twI = twt<T>(ctx, nin); a.twO = twt<T>(ctx, nout); a.pad_copy = 0; a.zero_nyq = 0; a.kmul = 0;
+        return a;
+    }
+
+    // ---- ddx / ddy (004_derivatives.f90:18-81) ----
+    int ddx(T *dfdx, const T *fun, int nlev)
+    {
+        auto a = rowargs(fun, ctx->ldx, dfdx, ctx->ldx, (long long)ctx->nyt * nlev, 1.0 / ctx->nxt, ctx->nxt, ctx->nxt);
+        a.ktab = ctx->d_kx;
+        return rows(OP_DERIV, ctx->nxt, a, "ddx_rows");
+    }
+    int ddy(T *dfdy, const T *fun, int nlev)
+    {
+        auto a = colargs(fun, ctx->ldx, ctx->plane(), dfdy, ctx->ldx, ctx->plane(), ctx->nxt, nlev,
+                         1.0 / ctx->nyt, ctx->nyt, ctx->nyt);
+        a.ktab = ctx->d_ky1;
+        return cols(OP_DERIV, true, ctx->nyt, a, "ddy_cols");
+    }
+
+    // ---- zero_padding / zero_unpadding (108_01_padd.f90:73-197) ----
+    int pad(const T *var, T *big, int nlev)
+    {
+        const int nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        int rc = ensure(ctx, ctx->tmp, sizeof(T) * (size_t)nx2 * ny * nlev);
+        if (rc) return rc;
+        T *xb = (T *)ctx->tmp.p;  // var_x_big (nxt2, nyt, nlev)
+        auto ra = rowargs(var, ctx->ldx, xb, nx2, (long long)ny * nlev, 1.0 / nx, nx, nx2);
+        if ((rc = rows(OP_PAD, nx, ra, "pad_rows"))) return rc;
+        auto ca = colargs(xb, nx2, (long long)nx2 * ny, big, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny, ny, ny2);
+        return cols(OP_PAD, true, ny, ca, "pad_cols");
+    }
+    int unpad(const T *big, T *var, int nlev)
+    {
+        const int nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        int rc = ensure(ctx, ctx->tmp, sizeof(T) * (size_t)nx * ny2 * nlev);
+        if (rc) return rc;
+        T *xs = (T *)ctx->tmp.p;  // var_x (nxt, nyt2, nlev)
+        auto ra = rowargs(big, nx2, xs, nx, (long long)ny2 * nlev, 1.0 / nx2, nx2, nx);
+        if ((rc = rows(OP_UNPAD, nx, ra, "unpad_rows"))) return rc;
+        auto ca = colargs(xs, nx, (long long)nx * ny2, var, ctx->ldx, ctx->plane(), nx, nlev, 1.0 / ny2, ny2, ny);
+        ca.pad_copy = 1;
+        return cols(OP_UNPAD, true, ny, ca, "unpad_cols");
+    }
+
+    // ---- fftn / ifftn (203_fftn_mpi.f90:4-67) ----
+    // real planes (ldx stride) -> complex planes (lhx stride), nlev planes
+    int fftn(const T *in, C2<T> *out, int nlev, double scale)
+    {
+        auto ra = rowargs(in, ctx->ldx, out, ctx->lhx, (long long)ctx->nyt * nlev, scale, ctx->nxt, ctx->nxt);
+        int rc = rows(OP_FWD, ctx->nxt, ra, "fftn_rows");
+        if (rc) return rc;
+        auto ca = colargs(out, ctx->lhx, ctx->sp(), out, ctx->lhx, ctx->sp(), ctx->lhx, nlev, 1.0, ctx->nyt, ctx->nyt);
+        ca.zero_nyq = 1;
+        return cols(OP_FWD, false, ctx->nyt, ca, "fftn_cols");
+    }
+    // complex planes -> real planes; tmp receives the y-inverse (may alias in when in is scratch)
+    int ifftn(const C2<T> *in, C2<T> *tmp, T *out, long long out_plane_off_unused, int nlev, int kmul,
+              T pad_scale = (T)1, int pad_mode = 0)
+    {
+        (void)out_plane_off_unused;
+        auto ca = colargs(in, ctx->lhx, ctx->sp(), tmp, ctx->lhx, ctx->sp(), ctx->lhx, nlev, 1.0, ctx->nyt, ctx->nyt);
+        ca.kmul = kmul;
+        ca.ktab = kmul == 1 ? ctx->d_kx : ctx->d_ky2;
+        int rc = cols(OP_INV, false, ctx->nyt, ca, "ifftn_cols");
+        if (rc) return rc;
+        auto ra = rowargs(tmp, ctx->lhx, out, ctx->ldx, (long long)ctx->nyt * nlev, 1.0, ctx->nxt, ctx->nxt);
+        ra.pad_scale = pad_scale;
+        ra.pad_mode = pad_mode;
+        return rows(OP_INV, ctx->nxt, ra, "ifftn_rows");
+    }
+
+    int filter(T *f, int nlev)
+    {
+        int rc = ensure(ctx, ctx->tmp, sizeof(C2<T>) * (size_t)ctx->sp() * nlev);
+        if (rc) return rc;
+        C2<T> *sp = (C2<T> *)ctx->tmp.p;
+        const double cst = 1.0 / ((double)ctx->nxt * ctx->nyt);   // 006_test_filter.f90:98
+        if ((rc = fftn(f, sp, nlev, cst))) return rc;
+        return ifftn(sp, sp, f, 0, nlev, 0, (T)cst, 1);
+    }
+
+    // ---- press_stag_array (109_press_stag_array.f90:107-240) ----
+    int press(const T *u, const T *v, const T *w, const T *dbot, const T *dtop, T *p, T *dpdx, T *dpdy)
+    {
+        const long long S = ctx->sp();
+        const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
+        int rc;
+        for (int i = 0; i < 4; ++i)
+            if ((rc = ensure(ctx, ctx->spec[i], sb))) return rc;
+        if ((rc = ensure(ctx, ctx->cscr, sizeof(T) * (size_t)S * ctx->L))) return rc;
+        C2<T> *Hx = (C2<T> *)ctx->spec[0].p, *Hy = (C2<T> *)ctx->spec[1].p, *Hz = (C2<T> *)ctx->spec[2].p,
+              *ph = (C2<T> *)ctx->spec[3].p;
+        const long long pl = ctx->plane();
+        const int L = ctx->L, nx = ctx->nxt, ny = ctx->nyt, lhx = ctx->lhx, ldx = ctx->ldx;
+        const double cst = 1.0 / ((double)nx * ny);               // :153
+        const double sc = (cst / kTadv1) * (1.0 / ctx->dt_nd);     // rH = const/tadv1*(u/dt) (:166-168)
+
+        // x r2c of levels 1..L of u, v, w straight into the spectral buffers
+        const T *src[3] = {u, v, w};
+        C2<T> *dst[3] = {Hx, Hy, Hz};
+        for (int c = 0; c < 3; ++c) {
+            auto ra = rowargs(src[c] + pl, ldx, dst[c] + S, lhx, (long long)ny * L, sc, nx, nx);
+            if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
+        }
+        // boundary planes H_z(0) and H_z(nz) (:186-200)
+        if (dbot) {
+            auto ra = rowargs(dbot, ldx, Hz, lhx, ny, cst, nx, nx);
+            if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
+        } else {
+            CK(cudaMemsetAsync(Hz, 0, sizeof(C2<T>) * S, s()));
+        }
+        if (ctx->opt.top_bc == OBL_TOP_NEUMANN && dtop) {
+            auto ra = rowargs(dtop, ldx, Hz + S * (L + 1), lhx, ny, cst, nx, nx);
+            if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
+        } else {
+            CK(cudaMemsetAsync(Hz + S * (L + 1), 0, sizeof(C2<T>) * S, s()));
+        }
+        // y c2c (in place), y-Nyquist zeroed
+        {
+            auto ca = colargs(Hx + S, lhx, S, Hx + S, lhx, S, lhx, L, 1.0, ny, ny);
+            ca.zero_nyq = 1;
+            if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
+            ca.src = ca.dst = Hy + S;
+            if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
+            ca.src = ca.dst = Hz;
+            ca.nlev = L + 2;
+            if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
+        }
+        // tridiagonal solve per (kx,ky) column
+        TdmaArgs<T> ta{};
+        ta.Hx = Hx; ta.Hy = Hy; ta.Hz = Hz; ta.phat = ph; ta.cscr = (T *)ctx->cscr.p;
+        ta.kx = ctx->d_kx; ta.ky = ctx->d_ky2; ta.skip = ctx->n_isl ? ctx->d_skip : nullptr;
+        ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz;
+        ta.neumann_top = ctx->opt.top_bc == OBL_TOP_NEUMANN;
+        {
+            cudaError_t e = cudaSuccess;
+            {
+                LaunchScope ls(ctx->rec, "tdma", s());
+                launch_tdma<T>(ta, s(), e);
+            }
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma");
+            if (ctx->n_isl) {
+                if ((rc = ensure(ctx, ctx->isl_c, sizeof(double) * (size_t)ctx->n_isl * L))) return rc;
+                if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
+                IslandArgs isl{ctx->d_isl, ctx->n_isl, (double *)ctx->isl_c.p, (double2 *)ctx->isl_d.p};
+                LaunchScope ls(ctx->rec, "tdma_fp64_islands", s());
+                launch_tdma_island<T>(ta, isl, s(), e);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_island");
+            }
+        }
+        // inverse transforms (:231-238): p at 0..L, dpdx/dpdy at 1..L; Hx/Hy/Hz are
+        // free now and hold the y-inverses
+        if ((rc = ifftn(ph, Hz, p, 0, L + 1, 0))) return rc;
+        if ((rc = ifftn(ph + S, Hx, dpdx, 0, L, 1))) return rc;
+        if ((rc = ifftn(ph + S, Hy, dpdy, 0, L, 2))) return rc;
+        return OBL_OK;
+    }
+
+    int dpdz(const T *p, T *dp)
+    {
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "dpdz", s());
+        launch_dpdz<T>(dp, p, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
+        return chk(e, "dpdz");
+    }
+    int project(T *u, T *v, T *w, const T *dpdx, const T *dpdy, const T *dpdz_)
+    {
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "project", s());
+        ctx->rec.launches += 1;   // project + boundary kernel
+        launch_project<T>(u, v, w, dpdx, dpdy, dpdz_, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dt_nd,
+                          ctx->opt.ubc_stress_free, s(), e);
+        return chk(e, "project");
+    }
+    int ddz_uv(T *d, const T *f)
+    {
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "ddz_uv", s());
+        launch_ddz_uv<T>(d, f, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
+        return chk(e, "ddz_uv");
+    }
+    int ddz_w(T *d, const T *f)
+    {
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "ddz_w", s());
+        launch_ddz_w<T>(d, f, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
+        return chk(e, "ddz_w");
+    }
+
+    // ---- the fused step ----
+    int step(const obl_step_io *io)
+    {
+        const int nlev = ctx->nz + 1;
+        const T *f[4] = {(const T *)io->u, (const T *)io->v, (const T *)io->w, (const T *)io->theta};
+        int rc;
+        for (int c = 0; c < 4; ++c) {
+            if ((rc = ddx((T *)io->d[2 * c], f[c], nlev))) return rc;
+            if ((rc = ddy((T *)io->d[2 * c + 1], f[c], nlev))) return rc;
+            if ((rc = pad(f[c], (T *)io->big[c], nlev))) return rc;
+        }
+        if ((rc = press(f[0], f[1], f[2], (const T *)io->divtz_bot, (const T *)io->divtz_top, (T *)io->p,
+                        (T *)io->dp[0], (T *)io->dp[1])))
+            return rc;
+        if ((rc = dpdz((const T *)io->p, (T *)io->dp[2]))) return rc;
+        return project((T *)io->u, (T *)io->v, (T *)io->w, (const T *)io->dp[0], (const T *)io->dp[1],
+                       (const T *)io->dp[2]);
+    }
+};
+
+// ----------------------------------------------------------------------------- host staging
+// An argument of a host-variant call: host pointer, element count, and which part the
+// reference routine writes (rows of nx of nrow rows at pitch ld, from row0), if any.
+struct HArg {
+    const void *h;
+    long long n;          // elements
+    bool in;              // copy host -> device before the call
+    bool out;             // copy the written region back
+    long long ld;         // row pitch (elements)
+    long long width;      // elements written per row
+    long long row0, nrows;
+};
+
+static HArg harg_in(const void *h, long long n) { return HArg{h, n, true, false, 0, 0, 0, 0}; }
+// output rows: x < width of rows [row0, row0+nrows) at pitch ld
+static HArg harg_out(const void *h, long long n, bool in, long long ld, long long width, long long row0,
+                     long long nrows)
+{
+    return HArg{h, n, in, true, ld, width, row0, nrows};
+}
+
+// Runs fn(device pointers) with every argument staged on the device in the storage
+// type; host arrays are double (HT = double) or float (HT = float).
+template <typename HT, class F> static int host_call(obl_ctx *ctx, std::vector<HArg> args, F fn)
+{
+    const size_t es = ctx->es();
+    if (ctx->stage.size() < args.size()) ctx->stage.resize(args.size());
+    if (ctx->stage64.size() < args.size()) ctx->stage64.resize(args.size());
+    std::vector<void *> dp(args.size(), nullptr);
+    const bool conv = (sizeof(HT) != es);
+    int rc;
+    for (size_t i = 0; i < args.size(); ++i) {
+        if (!args[i].h) continue;
+        if ((rc = ensure(ctx, ctx->stage[i], es * args[i].n))) return rc;
+        dp[i] = ctx->stage[i].p;
+        if (conv && (rc = ensure(ctx, ctx->stage64[i], sizeof(HT) * args[i].n))) return rc;
+    }
+    cudaStream_t s = ctx->stream;
+    for (size_t i = 0; i < args.size(); ++i) {
+        const HArg &a = args[i];
+        if (!a.h || !a.in) continue;
+        void *landing = conv ? ctx->stage64[i].p : dp[i];
+        CK(cudaMemcpyAsync(landing, a.h, sizeof(HT) * a.n, cudaMemcpyHostToDevice, s));
+        if (conv) {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "convert", s);
+            if (sizeof(HT) == 8) launch_convert_d2f((float *)dp[i], (const double *)landing, a.n, s, e);
+            else launch_convert_f2d((double *)dp[i], (const float *)landing, a.n, s, e);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "convert");
+        }
+    }
+    if ((rc = fn(dp))) return rc;
+    for (size_t i = 0; i < args.size(); ++i) {
+        const HArg &a = args[i];
+        if (!a.h || !a.out) continue;
+        const void *from = dp[i];
+        if (conv) {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "convert", s);
+            if (sizeof(HT) == 8) launch_convert_f2d((double *)ctx->stage64[i].p, (const float *)dp[i], a.n, s, e);
+            else launch_convert_d2f((float *)ctx->stage64[i].p, (const double *)dp[i], a.n, s, e);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "convert");
+            from = ctx->stage64[i].p;
+        }
+        const size_t hb = sizeof(HT);
+        char *hdst = (char *)a.h + hb * a.row0 * a.ld;
+        const char *dsrc = (const char *)from + hb * a.row0 * a.ld;
+        if (a.width == a.ld)
+            CK(cudaMemcpyAsync(hdst, dsrc, hb * a.ld * a.nrows, cudaMemcpyDeviceToHost, s));
+        else
+            CK(cudaMemcpy2DAsync(hdst, hb * a.ld, dsrc, hb * a.ld, hb * a.width, a.nrows, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return OBL_OK;
+}
+
+} // namespace
+
+// ============================================================================= C ABI
+extern "C" {
+
+int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
+{
+    if (!grid || !out) return OBL_ERR_ARG;
+    *out = nullptr;
+    obl_options o{};
+    o.precision = OBL_PREC_F64;
+    o.top_bc = OBL_TOP_NEUMANN;
+    o.fp64_k2_max = -1.0;
+    if (opt) o = *opt;
+    const obl_grid &g = *grid;
+    if (o.precision < 0 || o.precision > 2 || o.top_bc < 0 || o.top_bc > 1) return OBL_ERR_ARG;
+    if (g.nxt <= 0 || g.nyt <= 0 || g.nzt < 4 || !(g.lx_tot > 0) || !(g.ly_tot > 0) || !(g.lz_tot > 0) ||
+        !(g.z_i > 0) || !(g.dt > 0) || !(g.u_scale > 0))
+        return OBL_ERR_ARG;
+    if (!len_ok(g.nxt) || !len_ok(g.nyt)) return OBL_ERR_UNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return OBL_ERR_NODEV;
+    }
+    if (o.device < 0 || o.device >= ndev) return OBL_ERR_ARG;
+
+    obl_ctx *ctx = new obl_ctx();
+    ctx->grid = g;
+    ctx->opt = o;
+    ctx->dev = o.device;
+    ctx->f64 = (o.precision == OBL_PREC_F64);
+    // init_parameter (102_initial.f90:119-141) with npz = npy = 1
+    ctx->nxt = g.nxt;
+    ctx->nyt = g.nyt;
+    ctx->nzt = g.nzt;
+    ctx->nz = g.nzt;
+    ctx->L = g.nzt - 1;
+    ctx->lhx = g.nxt / 2 + 1;
+    ctx->lhy = g.nyt / 2 + 1;
+    ctx->ldx = 2 * ctx->lhx;
+    ctx->nxt2 = 3 * g.nxt / 2;
+    ctx->nyt2 = 3 * g.nyt / 2;
+    // init_nondimensional (102_initial.f90:186-199)
+    ctx->lx = g.lx_tot / g.z_i;
+    ctx->ly = g.ly_tot / g.z_i;
+    ctx->dz = (g.lz_tot / (double)(g.nzt - 1)) / g.z_i;
+    ctx->dt_nd = g.dt * g.u_scale / g.z_i;
+
+    auto bad = [&](int code) {
+        obl_ctx_destroy(ctx);
+        return code;
+    };
+    if (cudaSetDevice(ctx->dev) != cudaSuccess) return bad(OBL_ERR_CUDA);
+
+    // wavenumbers (002_fft.f90:131-165)
+    std::vector<double> kx(ctx->lhx), ky1(ctx->lhy), ky2(ctx->nyt);
+    for (int i = 0; i < ctx->lhx; ++i) kx[i] = (((double)i * 2.0) * kPi) / ctx->lx;
+    for (int i = 0; i < ctx->lhy; ++i) ky1[i] = (((double)i * 2.0) * kPi) / ctx->ly;
+    kx[ctx->lhx - 1] = 0.0;
+    ky1[ctx->lhy - 1] = 0.0;
+    for (int j = 0; j < ctx->nyt; ++j)
+        ky2[j] = (((double)(((j + ctx->nyt / 2) % ctx->nyt) - ctx->nyt / 2) * 2.0) * kPi) / ctx->ly;
+    ky2[ctx->nyt / 2] = 0.0;
+    auto upload = [&](double **d, const std::vector<double> &h) {
+        if (cudaMalloc(d, sizeof(double) * h.size()) != cudaSuccess) return false;
+        return cudaMemcpy(*d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (!upload(&ctx->d_kx, kx) || !upload(&ctx->d_ky1, ky1) || !upload(&ctx->d_ky2, ky2)) return bad(OBL_ERR_NOMEM);
+
+    // twiddle tables w_N^m = exp(-2 pi i m / N) for every transform length in use
+    for (int n : {ctx->nxt, ctx->nyt, ctx->nxt2, ctx->nyt2}) {
+        if (ctx->tw.count(n)) continue;
+        void *d = nullptr;
+        const size_t b = (ctx->f64 ? sizeof(double2) : sizeof(float2)) * (size_t)n;
+        if (cudaMalloc(&d, b) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+        ctx->tw[n] = d;
+        if (ctx->f64) {
+            std::vector<double2> h(n);
+            for (int m = 0; m < n; ++m) {
+                const double a = -2.0 * kPi * (double)m / (double)n;
+                h[m] = make_double2(std::cos(a), std::sin(a));
+            }
+            if (cudaMemcpy(d, h.data(), b, cudaMemcpyHostToDevice) != cudaSuccess) return bad(OBL_ERR_CUDA);
+        } else {
+            std::vector<float2> h(n);
+            for (int m = 0; m < n; ++m) {
+                const double a = -2.0 * kPi * (double)m / (double)n;
+                h[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+            }
+            if (cudaMemcpy(d, h.data(), b, cudaMemcpyHostToDevice) != cudaSuccess) return bad(OBL_ERR_CUDA);
+        }
+    }
+
+    // FP64 islands of the mixed mode: the (0,0) mean mode and every column with
+    // k^2 <= fp64_k2_max (weakly diagonally dominant systems)
+    if (o.precision == OBL_PREC_MIXED) {
+        double k2max = o.fp64_k2_max;
+        if (k2max < 0) k2max = (4.0 / (ctx->dz * ctx->dz)) / 16.0;
+        std::vector<int> cols;
+        std::vector<unsigned char> skip((size_t)ctx->lhx * ctx->nyt, 0);
+        for (int j = 0; j < ctx->nyt; ++j)
+            for (int i = 0; i < ctx->lhx; ++i) {
+                if (i == ctx->lhx - 1 || j == ctx->nyt / 2) continue;
+                const double k2 = kx[i] * kx[i] + ky2[j] * ky2[j];
+                if (k2 <= k2max) {
+                    cols.push_back(i + ctx->lhx * j);
+                    skip[(size_t)i + (size_t)ctx->lhx * j] = 1;
+                }
+            }
+        ctx->n_isl = (int)cols.size();
+        if (ctx->n_isl) {
+            if (cudaMalloc(&ctx->d_isl, sizeof(int) * cols.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            if (cudaMalloc(&ctx->d_skip, skip.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            cudaMemcpy(ctx->d_isl, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(ctx->d_skip, skip.data(), skip.size(), cudaMemcpyHostToDevice);
+        }
+    }
+    *out = ctx;
+    return OBL_OK;
+}
+
+int obl_ctx_destroy(obl_ctx *ctx)
+{
+    if (!ctx) return OBL_OK;
+    cudaSetDevice(ctx->dev);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    else cudaDeviceSynchronize();
+    cudaFree(ctx->d_kx);
+    cudaFree(ctx->d_ky1);
+    cudaFree(ctx->d_ky2);
+    cudaFree(ctx->d_isl);
+    cudaFree(ctx->d_skip);
+    for (auto &kv : ctx->tw) cudaFree(kv.second);
+    for (auto &b : ctx->spec) cudaFree(b.p);
+    cudaFree(ctx->cscr.p);
+    cudaFree(ctx->isl_c.p);
+    cudaFree(ctx->isl_d.p);
+    cudaFree(ctx->tmp.p);
+    for (auto &b : ctx->stage) cudaFree(b.p);
+    for (auto &b : ctx->stage64) cudaFree(b.p);
+    delete ctx;
+    return OBL_OK;
+}
+
+int obl_ctx_info(const obl_ctx *ctx, obl_info *info)
+{
+    if (!ctx || !info) return OBL_ERR_ARG;
+    info->nxt = ctx->nxt; info->nyt = ctx->nyt; info->nzt = ctx->nzt; info->nz = ctx->nz;
+    info->ldx = ctx->ldx; info->lhx = ctx->lhx; info->nxt2 = ctx->nxt2; info->nyt2 = ctx->nyt2;
+    info->elem_bytes = (int)ctx->es();
+    info->n_fp64_columns = ctx->n_isl;
+    info->dz = ctx->dz; info->dt_nd = ctx->dt_nd; info->lx = ctx->lx; info->ly = ctx->ly;
+    info->field_elems = ctx->field(); info->dfield_elems = ctx->dfield(); info->big_elems = ctx->big();
+    info->spec_elems = ctx->sp();
+    return OBL_OK;
+}
+
+int obl_set_stream(obl_ctx *ctx, void *stream)
+{
+    if (!ctx) return OBL_ERR_ARG;
+    ctx->stream = (cudaStream_t)stream;
+    return OBL_OK;
+}
+
+int obl_synchronize(obl_ctx *ctx)
+{
+    CTX_OK();
+    CK(cudaStreamSynchronize(ctx->stream));
+    return OBL_OK;
+}
+
+int obl_last_error(const obl_ctx *ctx, char *buf, size_t n)
+{
+    if (!ctx || !buf || n == 0) return OBL_ERR_ARG;
+    std::strncpy(buf, ctx->err.c_str(), n - 1);
+    buf[n - 1] = 0;
+    return OBL_OK;
+}
+
+long long obl_launch_count(const obl_ctx *ctx) { return ctx ? ctx->rec.launches : -1; }
+
+int obl_timing_enable(obl_ctx *ctx, int on)
+{
+    if (!ctx) return OBL_ERR_ARG;
+    ctx->rec.timing = on != 0;
+    return OBL_OK;
+}
+
+int obl_timing_report(obl_ctx *ctx, char *buf, size_t n)
+{
+    CTX_OK();
+    if (!buf || n == 0) return OBL_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::map<std::string, std::pair<long long, double>> agg;
+    for (auto &r : ctx->rec.recs) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) { cudaGetLastError(); continue; }
+        auto &x = agg[r.name];
+        x.first += 1;
+        x.second += ms;
+    }
+    ctx->rec.release();
+    std::string js = "{";
+    bool first = true;
+    for (auto &kv : agg) {
+        char tmp[256];
+        std::snprintf(tmp, sizeof tmp, "%s\"%s\": [%lld, %.6f]", first ? "" : ", ", kv.first.c_str(),
+                      kv.second.first, kv.second.second);
+        js += tmp;
+        first = false;
+    }
+    js += "}";
+    if (js.size() + 1 > n) return fail(ctx, OBL_ERR_ARG, "timing report buffer too small");
+    std::memcpy(buf, js.c_str(), js.size() + 1);
+    return OBL_OK;
+}
+
+} // extern "C"
+
+namespace {
+template <typename T> struct OpsT : Ops<T> { using Tt = T; };
+template <class F> static int dispatchT(obl_ctx *ctx, F fn)
+{
+    if (ctx->f64) {
+        OpsT<double> o{{ctx}};
+        return fn(o);
+    }
+    OpsT<float> o{{ctx}};
+    return fn(o);
+}
+} // namespace
+
+#define DEVCALL(ctx, body)                                                                         \
+    do {                                                                                           \
+        if (!ctx) return OBL_ERR_ARG;                                                              \
+        if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice"); \
+        return dispatchT(ctx, [&](auto &o) -> int {                                                \
+            using T = typename std::remove_reference<decltype(o)>::type::Tt;                       \
+            (void)sizeof(T);                                                                       \
+            body                                                                                   \
+        });                                                                                        \
+    } while (0)
+
+static bool nlev_ok(const obl_ctx *c, int nlev) { return nlev > 0 && ((long long)c->nyt * nlev) % 2 == 0; }
+
+extern "C" {
+
+int obl_ddx_dev(obl_ctx *ctx, void *dfdx, const void *fun, int nlev)
+{
+    if (!ctx || !dfdx || !fun || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.ddx((T *)dfdx, (const T *)fun, nlev););
+}
+int obl_ddy_dev(obl_ctx *ctx, void *dfdy, const void *fun, int nlev)
+{
+    if (!ctx || !dfdy || !fun || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.ddy((T *)dfdy, (const T *)fun, nlev););
+}
+int obl_ddz_uv_dev(obl_ctx *ctx, void *dfdz, const void *fun)
+{
+    if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.ddz_uv((T *)dfdz, (const T *)fun););
+}
+int obl_ddz_w_dev(obl_ctx *ctx, void *dfdz, const void *fun)
+{
+    if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.ddz_w((T *)dfdz, (const T *)fun););
+}
+int obl_fftn_dev(obl_ctx *ctx, const void *in, void *out, int nlev)
+{
+    if (!ctx || !in || !out || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.fftn((const T *)in, (C2<T> *)out, nlev, 1.0););
+}
+int obl_ifftn_dev(obl_ctx *ctx, const void *in, void *out, int nlev)
+{
+    if (!ctx || !in || !out || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    DEVCALL(ctx, {
+        int rc = ensure(ctx, ctx->tmp, sizeof(C2<T>) * (size_t)ctx->sp() * nlev);
+        if (rc) return rc;
+        return o.ifftn((const C2<T> *)in, (C2<T> *)ctx->tmp.p, (T *)out, 0, nlev, 0);
+    });
+}
+int obl_zero_padding_dev(obl_ctx *ctx, const void *var, void *big, int nlev)
+{
+    if (!ctx || !var || !big || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.pad((const T *)var, (T *)big, nlev););
+}
+int obl_zero_unpadding_dev(obl_ctx *ctx, const void *big, void *var, int nlev)
+{
+    if (!ctx || !var || !big || nlev <= 0) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.unpad((const T *)big, (T *)var, nlev););
+}
+int obl_filter_data_dev(obl_ctx *ctx, void *f, int nlev)
+{
+    if (!ctx || !f || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.filter((T *)f, nlev););
+}
+int obl_press_stag_array_dev(obl_ctx *ctx, const void *u, const void *v, const void *w, const void *dbot,
+                             const void *dtop, void *p, void *dpdx, void *dpdy)
+{
+    if (!ctx || !u || !v || !w || !p || !dpdx || !dpdy) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.press((const T *)u, (const T *)v, (const T *)w, (const T *)dbot, (const T *)dtop,
+                                (T *)p, (T *)dpdx, (T *)dpdy););
+}
+int obl_dpdz_dev(obl_ctx *ctx, const void *p, void *dpdz)
+{
+    if (!ctx || !p || !dpdz) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.dpdz((const T *)p, (T *)dpdz););
+}
+int obl_project_dev(obl_ctx *ctx, void *u, void *v, void *w, const void *dpdx, const void *dpdy,
+                    const void *dpdz)
+{
+    if (!ctx || !u || !v || !w || !dpdx || !dpdy || !dpdz) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.project((T *)u, (T *)v, (T *)w, (const T *)dpdx, (const T *)dpdy, (const T *)dpdz););
+}
+static bool step_io_ok(const obl_step_io *io)
+{
+    if (!io || !io->u || !io->v || !io->w || !io->theta || !io->p) return false;
+    for (int i = 0; i < 8; ++i)
+        if (!io->d[i]) return false;
+    for (int i = 0; i < 4; ++i)
+        if (!io->big[i]) return false;
+    for (int i = 0; i < 3; ++i)
+        if (!io->dp[i]) return false;
+    return true;
+}
+int obl_step_dev(obl_ctx *ctx, const obl_step_io *io)
+{
+    if (!ctx || !step_io_ok(io)) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.step(io););
+}
+
+// ---------------------------------------------------------------- host entry points
+#define HOSTCALL(HT, ctx, args, body)                                                              \
+    do {                                                                                           \
+        if (!ctx) return OBL_ERR_ARG;                                                              \
+        if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice"); \
+        return dispatchT(ctx, [&](auto &o) -> int {                                                \
+            using T = typename std::remove_reference<decltype(o)>::type::Tt;                       \
+            (void)sizeof(T);                                                                       \
+            return host_call<HT>(ctx, args, [&](std::vector<void *> &d) -> int { body });         \
+        });                                                                                        \
+    } while (0)
+
+int obl_ddx(obl_ctx *ctx, double *dfdx, const double *fun, int nlev)
+{
+    if (!ctx || !dfdx || !fun || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const long long n = ctx->plane() * nlev;
+    std::vector<HArg> a{harg_in(fun, n), harg_out(dfdx, n, false, ctx->ldx, ctx->nxt, 0, (long long)ctx->nyt * nlev)};
+    HOSTCALL(double, ctx, a, return o.ddx((T *)d[1], (const T *)d[0], nlev););
+}
+int obl_ddy(obl_ctx *ctx, double *dfdy, const double *fun, int nlev)
+{
+    if (!ctx || !dfdy || !fun || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const long long n = ctx->plane() * nlev;
+    std::vector<HArg> a{harg_in(fun, n), harg_out(dfdy, n, false, ctx->ldx, ctx->nxt, 0, (long long)ctx->nyt * nlev)};
+    HOSTCALL(double, ctx, a, return o.ddy((T *)d[1], (const T *)d[0], nlev););
+}
+int obl_ddz_uv(obl_ctx *ctx, double *dfdz, const double *fun)
+{
+    if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
+    const long long n = ctx->field(), nyt = ctx->nyt;
+    // level 0 (all ldx) and levels 2..nz-1 (x < nxt): copy the device result of the
+    // whole array back after staging the host output too, so untouched levels survive
+    std::vector<HArg> a{harg_in(fun, n), harg_out(dfdz, n, true, ctx->ldx, ctx->ldx, 0, nyt * (ctx->nz + 1))};
+    HOSTCALL(double, ctx, a, return o.ddz_uv((T *)d[1], (const T *)d[0]););
+}
+int obl_ddz_w(obl_ctx *ctx, double *dfdz, const double *fun)
+{
+    if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
+    const long long n = ctx->field(), nyt = ctx->nyt;
+    std::vector<HArg> a{harg_in(fun, n), harg_out(dfdz, n, true, ctx->ldx, ctx->ldx, 0, nyt * (ctx->nz + 1))};
+    HOSTCALL(double, ctx, a, return o.ddz_w((T *)d[1], (const T *)d[0]););
+}
+int obl_fftn(obl_ctx *ctx, const double *in, double *out, int nlev)
+{
+    if (!ctx || !in || !out || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const long long ni = ctx->plane() * nlev, no = 2 * ctx->sp() * nlev;
+    std::vector<HArg> a{harg_in(in, ni), harg_out(out, no, false, no, no, 0, 1)};
+    HOSTCALL(double, ctx, a, return o.fftn((const T *)d[0], (C2<T> *)d[1], nlev, 1.0););
+}
+int obl_ifftn(obl_ctx *ctx, const double *in, double *out, int nlev)
+{
+    if (!ctx || !in || !out || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const long long ni = 2 * ctx->sp() * nlev, no = ctx->plane() * nlev;
+    std::vector<HArg> a{harg_in(in, ni), harg_out(out, no, false, ctx->ldx, ctx->nxt, 0, (long long)ctx->nyt * nlev)};
+    HOSTCALL(double, ctx, a, {
+        int rc = ensure(ctx, ctx->tmp, sizeof(C2<T>) * (size_t)ctx->sp() * nlev);
+        if (rc) return rc;
+        return o.ifftn((const C2<T> *)d[0], (C2<T> *)ctx->tmp.p, (T *)d[1], 0, nlev, 0);
+    });
+}
+int obl_zero_padding(obl_ctx *ctx, const double *var, double *big, int nlev)
+{
+    if (!ctx || !var || !big || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const long long ni = ctx->plane() * nlev, no = (long long)ctx->nxt2 * ctx->nyt2 * nlev;
+    std::vector<HArg> a{harg_in(var, ni), harg_out(big, no, false, no, no, 0, 1)};
+    HOSTCALL(double, ctx, a, return o.pad((const T *)d[0], (T *)d[1], nlev););
+}
+int obl_zero_unpadding(obl_ctx *ctx, const double *big, double *var, int nlev)
+{
+    if (!ctx || !var || !big || nlev <= 0) return OBL_ERR_ARG;
+    const long long ni = (long long)ctx->nxt2 * ctx->nyt2 * nlev, no = ctx->plane() * nlev;
+    std::vector<HArg> a{harg_in(big, ni), harg_out(var, no, false, no, no, 0, 1)};
+    HOSTCALL(double, ctx, a, return o.unpad((const T *)d[0], (T *)d[1], nlev););
+}
+int obl_filter_data(obl_ctx *ctx, double *f, int nlev)
+{
+    if (!ctx || !f || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const long long n = ctx->plane() * nlev;
+    std::vector<HArg> a{harg_out(f, n, true, n, n, 0, 1)};
+    HOSTCALL(double, ctx, a, return o.filter((T *)d[0], nlev););
+}
+int obl_press_stag_array(obl_ctx *ctx, const double *u, const double *v, const double *w,
+                         const double *dbot, const double *dtop, double *p, double *dpdx, double *dpdy)
+{
+    if (!ctx || !u || !v || !w || !p || !dpdx || !dpdy) return OBL_ERR_ARG;
+    const long long nf = ctx->field(), nd = ctx->dfield(), pl = ctx->plane(), ny = ctx->nyt, L = ctx->L;
+    std::vector<HArg> a{harg_in(u, nf), harg_in(v, nf), harg_in(w, nf),
+                        dbot ? harg_in(dbot, pl) : HArg{nullptr, 0, false, false, 0, 0, 0, 0},
+                        dtop ? harg_in(dtop, pl) : HArg{nullptr, 0, false, false, 0, 0, 0, 0},
+                        harg_out(p, nf, false, ctx->ldx, ctx->nxt, 0, ny * (L + 1)),
+                        harg_out(dpdx, nd, false, ctx->ldx, ctx->nxt, 0, ny * L),
+                        harg_out(dpdy, nd, false, ctx->ldx, ctx->nxt, 0, ny * L)};
+    HOSTCALL(double, ctx, a,
+             return o.press((const T *)d[0], (const T *)d[1], (const T *)d[2], (const T *)d[3], (const T *)d[4],
+                            (T *)d[5], (T *)d[6], (T *)d[7]););
+}
+int obl_dpdz(obl_ctx *ctx, const double *p, double *dpdz)
+{
+    if (!ctx || !p || !dpdz) return OBL_ERR_ARG;
+    const long long nf = ctx->field(), nd = ctx->dfield(), ny = ctx->nyt;
+    std::vector<HArg> a{harg_in(p, nf), harg_out(dpdz, nd, false, ctx->ldx, ctx->nxt, 0, ny * ctx->L)};
+    HOSTCALL(double, ctx, a, return o.dpdz((const T *)d[0], (T *)d[1]););
+}
+int obl_project(obl_ctx *ctx, double *u, double *v, double *w, const double *dpdx, const double *dpdy,
+                const double *dpdz)
+{
+    if (!ctx || !u || !v || !w || !dpdx || !dpdy || !dpdz) return OBL_ERR_ARG;
+    const long long nf = ctx->field(), nd = ctx->dfield();
+    std::vector<HArg> a{harg_out(u, nf, true, nf, nf, 0, 1), harg_out(v, nf, true, nf, nf, 0, 1),
+                        harg_out(w, nf, true, nf, nf, 0, 1), harg_in(dpdx, nd), harg_in(dpdy, nd),
+                        harg_in(dpdz, nd)};
+    HOSTCALL(double, ctx, a,
+             return o.project((T *)d[0], (T *)d[1], (T *)d[2], (const T *)d[3], (const T *)d[4], (const T *)d[5]););
+}
+
+} // extern "C"
+
+template <typename HT> static int step_host(obl_ctx *ctx, const obl_step_io *io)
+{
+    const long long nf = ctx->field(), nd = ctx->dfield(), nb = ctx->big(), pl = ctx->plane(), ny = ctx->nyt;
+    const long long L = ctx->L, nlev = ctx->nz + 1;
+    std::vector<HArg> a;
+    a.push_back(harg_out(io->u, nf, true, nf, nf, 0, 1));
+    a.push_back(harg_out(io->v, nf, true, nf, nf, 0, 1));
+    a.push_back(harg_out(io->w, nf, true, nf, nf, 0, 1));
+    a.push_back(harg_in(io->theta, nf));
+    for (int i = 0; i < 8; ++i) a.push_back(harg_out(io->d[i], nf, false, ctx->ldx, ctx->nxt, 0, ny * nlev));
+    for (int i = 0; i < 4; ++i) a.push_back(harg_out(io->big[i], nb, false, nb, nb, 0, 1));
+    a.push_back(harg_out(io->p, nf, false, ctx->ldx, ctx->nxt, 0, ny * (L + 1)));
+    for (int i = 0; i < 3; ++i) a.push_back(harg_out(io->dp[i], nd, false, ctx->ldx, ctx->nxt, 0, ny * L));
+    a.push_back(io->divtz_bot ? harg_in(io->divtz_bot, pl) : HArg{nullptr, 0, false, false, 0, 0, 0, 0});
+    a.push_back(io->divtz_top ? harg_in(io->divtz_top, pl) : HArg{nullptr, 0, false, false, 0, 0, 0, 0});
+    if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice");
+    return dispatchT(ctx, [&](auto &o) -> int {
+        return host_call<HT>(ctx, a, [&](std::vector<void *> &d) -> int {
+            obl_step_io dio{};
+            dio.u = d[0]; dio.v = d[1]; dio.w = d[2]; dio.theta = d[3];
+            for (int i = 0; i < 8; ++i) dio.d[i] = d[4 + i];
+            for (int i = 0; i < 4; ++i) dio.big[i] = d[12 + i];
+            dio.p = d[16];
+            for (int i = 0; i < 3; ++i) dio.dp[i] = d[17 + i];
+            dio.divtz_bot = d[20];
+            dio.divtz_top = d[21];
+            return o.step(&dio);
+        });
+    });
+}
+
+extern "C" {
+
+int obl_step(obl_ctx *ctx, const obl_step_io *io)
+{
+    if (!ctx || !step_io_ok(io)) return OBL_ERR_ARG;
+    return step_host<double>(ctx, io);
+}
+int obl_step_f32(obl_ctx *ctx, const obl_step_io *io)
+{
+    if (!ctx || !step_io_ok(io)) return OBL_ERR_ARG;
+    return step_host<float>(ctx, io);
+}
+
+} // extern "C"

@@ -1,0 +1,62 @@
+// lines_dispatch.cuh -- runtime-length dispatch of the row / column kernels.
+// Supported base lengths n (and their 3/2 partners): the grid sizes of the
+// reference's production namelists and of the benchmark workloads.
+#pragma once
+#include "lines.cuh"
+
+#define OBL_FOR_EACH_N(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+
+namespace obl {
+
+template <typename T, int N>
+cudaError_t rows_n(int op, const RowArgs<T> &a, cudaStream_t s)
+{
+    switch (op) {
+    case OP_DERIV: return launch_rows_t<T, N, N, OP_DERIV>(a, s);
+    case OP_PAD: return launch_rows_t<T, N, 3 * N / 2, OP_PAD>(a, s);
+    case OP_UNPAD: return launch_rows_t<T, 3 * N / 2, N, OP_UNPAD>(a, s);
+    case OP_FWD: return launch_rows_t<T, N, N, OP_FWD>(a, s);
+    case OP_INV: return launch_rows_t<T, N, N, OP_INV>(a, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T, int N>
+cudaError_t cols_n(int op, bool real, const ColArgs<T> &a, cudaStream_t s)
+{
+    if (real) {
+        switch (op) {
+        case OP_DERIV: return launch_cols_t<T, N, N, OP_DERIV, true>(a, s);
+        case OP_PAD: return launch_cols_t<T, N, 3 * N / 2, OP_PAD, true>(a, s);
+        case OP_UNPAD: return launch_cols_t<T, 3 * N / 2, N, OP_UNPAD, true>(a, s);
+        }
+    } else {
+        switch (op) {
+        case OP_FWD: return launch_cols_t<T, N, N, OP_FWD, false>(a, s);
+        case OP_INV: return launch_cols_t<T, N, N, OP_INV, false>(a, s);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T> cudaError_t launch_rows(int op, int n, const RowArgs<T> &a, cudaStream_t s)
+{
+    switch (n) {
+#define OBL_CASE(N) case N: return rows_n<T, N>(op, a, s);
+        OBL_FOR_EACH_N(OBL_CASE)
+#undef OBL_CASE
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T> cudaError_t launch_cols(int op, bool real, int n, const ColArgs<T> &a, cudaStream_t s)
+{
+    switch (n) {
+#define OBL_CASE(N) case N: return cols_n<T, N>(op, real, a, s);
+        OBL_FOR_EACH_N(OBL_CASE)
+#undef OBL_CASE
+    }
+    return cudaErrorInvalidValue;
+}
+
+} // namespace obl

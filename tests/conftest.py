@@ -1,0 +1,50 @@
+"""pytest configuration: the `gpu` marker and shared fixtures.
+
+CPU tests (``-m "not gpu"``) exercise the FP64 oracle, its golden fixtures and the
+C-ABI library's loading and argument checks.  GPU tests (``-m gpu``) compare the
+CUDA path of libobl_b200.so with the oracle through the C ABI.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libobl_b200.so")
+
+
+def gpu_present():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if gpu_present():
+        return
+    skip = pytest.mark.skip(reason="no CUDA GPU in this environment")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)
+
+
+@pytest.fixture(scope="session")
+def orc():
+    from oracle import orc as _orc
+    _orc.lib()
+    return _orc
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64)
+    nb = np.linalg.norm(np.asarray(b).ravel())
+    d = np.linalg.norm((a - b).ravel())
+    return d / nb if nb > 0 else d

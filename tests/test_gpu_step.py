@@ -1,0 +1,57 @@
+"""GPU parity of the fused projection-plus-derivative step (obl_step) against the
+oracle's composition of the reference routines, and size-independent properties of
+the step at the headline size."""
+import numpy as np
+import pytest
+
+import overlappingbls_b200 as obl
+from overlappingbls_b200 import fields
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": 1e-12, "mixed": 1e-5}
+
+
+def _alloc_step(ctx, dtype=np.float64):
+    d = [ctx.field(dtype=dtype) for _ in range(8)]
+    big = [ctx.big_field(dtype=dtype) for _ in range(4)]
+    return d, big, ctx.field(dtype=dtype), [ctx.dfield(dtype=dtype) for _ in range(3)]
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("top,npz", [("neumann", 2), ("single", 1)])
+def test_step_matches_oracle(orc, prec, top, npz):
+    nx, ny, nzt = 64, 64, 65
+    ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
+    f = fields.make_fields(nx, ny, nzt)
+    u, v, w = (f[k].copy(order="F") for k in "uvw")
+    d, big, p, dp = _alloc_step(ctx)
+    ctx.step(u, v, w, f["theta"], d, big, p, dp)
+    ref = g.step(f["u"], f["v"], f["w"], f["theta"], npz=npz)
+    L = g.nz - 1
+    for i in range(8):
+        assert rel_l2(d[i][:nx], ref["d"][i][:nx]) < TOL[prec], i
+    for i in range(4):
+        assert rel_l2(big[i], ref["big"][i]) < TOL[prec], i
+    assert rel_l2(p[:nx, :, : L + 1], ref["p"][:nx, :, : L + 1]) < TOL[prec]
+    for a, k in zip(dp, ("dpdx", "dpdy", "dpdz")):
+        assert rel_l2(a[:nx, :, :L], ref[k][:nx, :, :L]) < TOL[prec], k
+    for a, k in ((u, "u"), (v, "v"), (w, "w")):
+        assert rel_l2(a, ref[k]) < TOL[prec], k
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+def test_step_f32_host_arrays(orc, prec):
+    nx, ny, nzt = 64, 64, 33
+    ctx = obl.Context(nx, ny, nzt, precision=prec, **fields.DOMAIN)
+    f = fields.make_fields(nx, ny, nzt)
+    u64, v64, w64 = (f[k].copy(order="F") for k in "uvw")
+    d, big, p, dp = _alloc_step(ctx)
+    ctx.step(u64, v64, w64, f["theta"], d, big, p, dp)
+    u32, v32, w32 = (f[k].astype(np.float32, order="F") for k in "uvw")
+    d32, big32, p32, dp32 = _alloc_step(ctx, np.float32)
+    ctx.step(u32, v32, w32, f["theta"].astype(np.float32, order="F"), d32, big32, p32, dp32)
+    assert rel_l2(p32[:nx], p[:nx]) < 1e-5
+    assert rel_l2(w32, w64) < 1e-5
