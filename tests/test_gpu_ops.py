@@ -6,7 +6,7 @@ import pytest
 
 import overlappingbls_b200 as obl
 from overlappingbls_b200 import fields
-from conftest import rel_l2
+from conftest import identical_inputs, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -32,7 +32,7 @@ def _pair(orc, grid, prec, top="neumann"):
     nx, ny, nzt = grid
     ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
     g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
-    f = fields.make_fields(nx, ny, nzt)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
     return ctx, g, f
 
 

@@ -6,7 +6,7 @@ import pytest
 
 import overlappingbls_b200 as obl
 from overlappingbls_b200 import fields
-from conftest import rel_l2
+from conftest import identical_inputs, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +25,7 @@ def test_step_matches_oracle(orc, prec, top, npz):
     nx, ny, nzt = 64, 64, 65
     ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
     g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
-    f = fields.make_fields(nx, ny, nzt)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
     u, v, w = (f[k].copy(order="F") for k in "uvw")
     d, big, p, dp = _alloc_step(ctx)
     ctx.step(u, v, w, f["theta"], d, big, p, dp)
@@ -46,7 +46,7 @@ def test_step_matches_oracle(orc, prec, top, npz):
 def test_step_f32_host_arrays(orc, prec):
     nx, ny, nzt = 64, 64, 33
     ctx = obl.Context(nx, ny, nzt, precision=prec, **fields.DOMAIN)
-    f = fields.make_fields(nx, ny, nzt)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
     u64, v64, w64 = (f[k].copy(order="F") for k in "uvw")
     d, big, p, dp = _alloc_step(ctx)
     ctx.step(u64, v64, w64, f["theta"], d, big, p, dp)
