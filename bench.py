@@ -31,6 +31,7 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # name: (nxt, nyt, nzt)
     "512x512x256": (512, 512, 257),
+    "512x512x64": (512, 512, 65),     # small case of the headline planes, for ncu captures
     "256x256x128": (256, 256, 129),
     "128x128x128": (128, 128, 129),
     "64x64x64": (64, 64, 65),
