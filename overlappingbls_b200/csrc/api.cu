@@ -41,13 +41,13 @@ struct obl_ctx {
     double *d_kx = nullptr;    // kx(lhx), Nyquist 0
     double *d_ky1 = nullptr;   // ky(lhy), Nyquist 0 (1D, for ddy)
     double *d_ky2 = nullptr;   // ky_2d row (nyt), Nyquist row 0
-    std::map<int, void *> tw;  // length -> w_N^m table in the storage precision
+    std::map<int, void *> tw;  // 4*n + role -> plan twiddle table in the storage precision
     // FP64 islands (mixed mode)
     int n_isl = 0;
     int *d_isl = nullptr;
     unsigned char *d_skip = nullptr;
     // work buffers
-    DevBuf spec[4];            // Hx, Hy, Hz, phat (lhx*nyt*(nz+1) complex)
+    DevBuf spec[5];            // Hx, Hy, Hz, phat, dpdz spectrum (lhx*nyt*(nz+1) complex)
     DevBuf cscr;               // c' scratch
     DevBuf isl_c, isl_d;
     DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
@@ -98,15 +98,12 @@ static int ensure(obl_ctx *ctx, DevBuf &b, size_t bytes)
     return OBL_OK;
 }
 
-template <typename T> static const C2<T> *twt(obl_ctx *c, int n) { return (const C2<T> *)c->tw.at(n); }
-
-static bool len_ok(int n)
+template <typename T> static const C2<T> *twt(obl_ctx *c, int n, int role)
 {
-    switch (n) {
-    case 32: case 48: case 64: case 96: case 128: case 192: case 256: case 384: case 512: return true;
-    }
-    return false;
+    return (const C2<T> *)c->tw.at(4 * n + role);
 }
+
+static bool len_ok(int n) { return line_length_supported(n); }
 
 // ----------------------------------------------------------------------------- typed ops
 namespace {
@@ -128,36 +125,46 @@ template <typename T> struct Ops {
         return chk(launch_cols<T>(op, real, n, a, s()), name);
     }
 
+    // plan twiddle tables of the forward / backward transform of a line op of base length n
+    void tables(int op, int n, const C2<T> *&f, const C2<T> *&b)
+    {
+        const int rf = op == OP_UNPAD ? ROLE_PADFWD : ROLE_FWD;
+        const int rb = op == OP_PAD ? ROLE_PADBWD : ROLE_BWD;
+        f = twt<T>(ctx, n, rf);
+        b = twt<T>(ctx, n, rb);
+    }
     RowArgs<T> rowargs(const void *src, long long ss, void *dst, long long ds, long long nrows, double scale,
-                       int nin, int nout)
+                       int op, int n)
     {
         RowArgs<T> a{};
         a.src = src; a.dst = dst; a.src_stride = ss; a.dst_stride = ds; a.npairs = nrows / 2;
-        a.scale = (T)scale; a.ktab = ctx->d_kx; a.twI = twt<T>(ctx, nin); a.twO = twt<T>(ctx, nout);
+        a.scale = (T)scale; a.ktab = ctx->d_kx;
+        tables(op, n, a.twF, a.twB);
         a.pad_scale = (T)1; a.pad_mode = 0;
         return a;
     }
     ColArgs<T> colargs(const void *src, long long srow, long long spl, void *dst, long long drow, long long dpl,
-                       int ncols, int nlev, double scale, int nin, int nout)
+                       int ncols, int nlev, double scale, int op, int n)
     {
         ColArgs<T> a{};
         a.src = src; a.dst = dst; a.src_row = srow; a.dst_row = drow; a.src_plane = spl; a.dst_plane = dpl;
         a.ncols = ncols; a.nlev = nlev; a.scale = (T)scale; a.ktab = ctx->d_ky1;
-        a.twI = twt<T>(ctx, nin); a.twO = twt<T>(ctx, nout); a.pad_copy = 0; a.zero_nyq = 0; a.kmul = 0;
+        tables(op, n, a.twF, a.twB);
+        a.pad_copy = 0; a.zero_nyq = 0; a.kmul = 0;
         return a;
     }
 
     // ---- ddx / ddy (004_derivatives.f90:18-81) ----
     int ddx(T *dfdx, const T *fun, int nlev)
     {
-        auto a = rowargs(fun, ctx->ldx, dfdx, ctx->ldx, (long long)ctx->nyt * nlev, 1.0 / ctx->nxt, ctx->nxt, ctx->nxt);
+        auto a = rowargs(fun, ctx->ldx, dfdx, ctx->ldx, (long long)ctx->nyt * nlev, 1.0 / ctx->nxt, OP_DERIV, ctx->nxt);
         a.ktab = ctx->d_kx;
         return rows(OP_DERIV, ctx->nxt, a, "ddx_rows");
     }
     int ddy(T *dfdy, const T *fun, int nlev)
     {
         auto a = colargs(fun, ctx->ldx, ctx->plane(), dfdy, ctx->ldx, ctx->plane(), ctx->nxt, nlev,
-                         1.0 / ctx->nyt, ctx->nyt, ctx->nyt);
+                         1.0 / ctx->nyt, OP_DERIV, ctx->nyt);
         a.ktab = ctx->d_ky1;
         return cols(OP_DERIV, true, ctx->nyt, a, "ddy_cols");
     }
@@ -169,9 +176,9 @@ template <typename T> struct Ops {
         int rc = ensure(ctx, ctx->tmp, sizeof(T) * (size_t)nx2 * ny * nlev);
         if (rc) return rc;
         T *xb = (T *)ctx->tmp.p;  // var_x_big (nxt2, nyt, nlev)
-        auto ra = rowargs(var, ctx->ldx, xb, nx2, (long long)ny * nlev, 1.0 / nx, nx, nx2);
+        auto ra = rowargs(var, ctx->ldx, xb, nx2, (long long)ny * nlev, 1.0 / nx, OP_PAD, nx);
         if ((rc = rows(OP_PAD, nx, ra, "pad_rows"))) return rc;
-        auto ca = colargs(xb, nx2, (long long)nx2 * ny, big, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny, ny, ny2);
+        auto ca = colargs(xb, nx2, (long long)nx2 * ny, big, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny, OP_PAD, ny);
         return cols(OP_PAD, true, ny, ca, "pad_cols");
     }
     int unpad(const T *big, T *var, int nlev)
@@ -180,9 +187,9 @@ template <typename T> struct Ops {
         int rc = ensure(ctx, ctx->tmp, sizeof(T) * (size_t)nx * ny2 * nlev);
         if (rc) return rc;
         T *xs = (T *)ctx->tmp.p;  // var_x (nxt, nyt2, nlev)
-        auto ra = rowargs(big, nx2, xs, nx, (long long)ny2 * nlev, 1.0 / nx2, nx2, nx);
+        auto ra = rowargs(big, nx2, xs, nx, (long long)ny2 * nlev, 1.0 / nx2, OP_UNPAD, nx);
         if ((rc = rows(OP_UNPAD, nx, ra, "unpad_rows"))) return rc;
-        auto ca = colargs(xs, nx, (long long)nx * ny2, var, ctx->ldx, ctx->plane(), nx, nlev, 1.0 / ny2, ny2, ny);
+        auto ca = colargs(xs, nx, (long long)nx * ny2, var, ctx->ldx, ctx->plane(), nx, nlev, 1.0 / ny2, OP_UNPAD, ny);
         ca.pad_copy = 1;
         return cols(OP_UNPAD, true, ny, ca, "unpad_cols");
     }
@@ -191,10 +198,10 @@ template <typename T> struct Ops {
     // real planes (ldx stride) -> complex planes (lhx stride), nlev planes
     int fftn(const T *in, C2<T> *out, int nlev, double scale)
     {
-        auto ra = rowargs(in, ctx->ldx, out, ctx->lhx, (long long)ctx->nyt * nlev, scale, ctx->nxt, ctx->nxt);
+        auto ra = rowargs(in, ctx->ldx, out, ctx->lhx, (long long)ctx->nyt * nlev, scale, OP_FWD, ctx->nxt);
         int rc = rows(OP_FWD, ctx->nxt, ra, "fftn_rows");
         if (rc) return rc;
-        auto ca = colargs(out, ctx->lhx, ctx->sp(), out, ctx->lhx, ctx->sp(), ctx->lhx, nlev, 1.0, ctx->nyt, ctx->nyt);
+        auto ca = colargs(out, ctx->lhx, ctx->sp(), out, ctx->lhx, ctx->sp(), ctx->lhx, nlev, 1.0, OP_FWD, ctx->nyt);
         ca.zero_nyq = 1;
         return cols(OP_FWD, false, ctx->nyt, ca, "fftn_cols");
     }
@@ -203,12 +210,12 @@ template <typename T> struct Ops {
               T pad_scale = (T)1, int pad_mode = 0)
     {
         (void)out_plane_off_unused;
-        auto ca = colargs(in, ctx->lhx, ctx->sp(), tmp, ctx->lhx, ctx->sp(), ctx->lhx, nlev, 1.0, ctx->nyt, ctx->nyt);
+        auto ca = colargs(in, ctx->lhx, ctx->sp(), tmp, ctx->lhx, ctx->sp(), ctx->lhx, nlev, 1.0, OP_INV, ctx->nyt);
         ca.kmul = kmul;
         ca.ktab = kmul == 1 ? ctx->d_kx : ctx->d_ky2;
         int rc = cols(OP_INV, false, ctx->nyt, ca, "ifftn_cols");
         if (rc) return rc;
-        auto ra = rowargs(tmp, ctx->lhx, out, ctx->ldx, (long long)ctx->nyt * nlev, 1.0, ctx->nxt, ctx->nxt);
+        auto ra = rowargs(tmp, ctx->lhx, out, ctx->ldx, (long long)ctx->nyt * nlev, 1.0, OP_INV, ctx->nxt);
         ra.pad_scale = pad_scale;
         ra.pad_mode = pad_mode;
         return rows(OP_INV, ctx->nxt, ra, "ifftn_rows");
@@ -225,12 +232,16 @@ template <typename T> struct Ops {
     }
 
     // ---- press_stag_array (109_press_stag_array.f90:107-240) ----
-    int press(const T *u, const T *v, const T *w, const T *dbot, const T *dtop, T *p, T *dpdx, T *dpdy)
+    // dpdz (optional): also return dpdz = ifftn((p_hat(z) - p_hat(z-1))/dz), the
+    // spectral form of the flosol difference (103_flosol.f90:174-175), whose
+    // z-difference is taken inside the solve in its own precision
+    int press(const T *u, const T *v, const T *w, const T *dbot, const T *dtop, T *p, T *dpdx, T *dpdy,
+              T *dpdz_out = nullptr)
     {
         const long long S = ctx->sp();
         const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
         int rc;
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < (dpdz_out ? 5 : 4); ++i)
             if ((rc = ensure(ctx, ctx->spec[i], sb))) return rc;
         if ((rc = ensure(ctx, ctx->cscr, sizeof(T) * (size_t)S * ctx->L))) return rc;
         C2<T> *Hx = (C2<T> *)ctx->spec[0].p, *Hy = (C2<T> *)ctx->spec[1].p, *Hz = (C2<T> *)ctx->spec[2].p,
@@ -244,25 +255,25 @@ template <typename T> struct Ops {
         const T *src[3] = {u, v, w};
         C2<T> *dst[3] = {Hx, Hy, Hz};
         for (int c = 0; c < 3; ++c) {
-            auto ra = rowargs(src[c] + pl, ldx, dst[c] + S, lhx, (long long)ny * L, sc, nx, nx);
+            auto ra = rowargs(src[c] + pl, ldx, dst[c] + S, lhx, (long long)ny * L, sc, OP_FWD, nx);
             if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
         }
         // boundary planes H_z(0) and H_z(nz) (:186-200)
         if (dbot) {
-            auto ra = rowargs(dbot, ldx, Hz, lhx, ny, cst, nx, nx);
+            auto ra = rowargs(dbot, ldx, Hz, lhx, ny, cst, OP_FWD, nx);
             if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
         } else {
             CK(cudaMemsetAsync(Hz, 0, sizeof(C2<T>) * S, s()));
         }
         if (ctx->opt.top_bc == OBL_TOP_NEUMANN && dtop) {
-            auto ra = rowargs(dtop, ldx, Hz + S * (L + 1), lhx, ny, cst, nx, nx);
+            auto ra = rowargs(dtop, ldx, Hz + S * (L + 1), lhx, ny, cst, OP_FWD, nx);
             if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
         } else {
             CK(cudaMemsetAsync(Hz + S * (L + 1), 0, sizeof(C2<T>) * S, s()));
         }
         // y c2c (in place), y-Nyquist zeroed
         {
-            auto ca = colargs(Hx + S, lhx, S, Hx + S, lhx, S, lhx, L, 1.0, ny, ny);
+            auto ca = colargs(Hx + S, lhx, S, Hx + S, lhx, S, lhx, L, 1.0, OP_FWD, ny);
             ca.zero_nyq = 1;
             if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
             ca.src = ca.dst = Hy + S;
@@ -276,6 +287,7 @@ template <typename T> struct Ops {
         ta.Hx = Hx; ta.Hy = Hy; ta.Hz = Hz; ta.phat = ph; ta.cscr = (T *)ctx->cscr.p;
         ta.kx = ctx->d_kx; ta.ky = ctx->d_ky2; ta.skip = ctx->n_isl ? ctx->d_skip : nullptr;
         ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz;
+        ta.dph = dpdz_out ? (C2<T> *)ctx->spec[4].p : nullptr;
         ta.neumann_top = ctx->opt.top_bc == OBL_TOP_NEUMANN;
         {
             cudaError_t e = cudaSuccess;
@@ -298,6 +310,10 @@ template <typename T> struct Ops {
         if ((rc = ifftn(ph, Hz, p, 0, L + 1, 0))) return rc;
         if ((rc = ifftn(ph + S, Hx, dpdx, 0, L, 1))) return rc;
         if ((rc = ifftn(ph + S, Hy, dpdy, 0, L, 2))) return rc;
+        if (dpdz_out) {
+            C2<T> *dph = (C2<T> *)ctx->spec[4].p + S;
+            if ((rc = ifftn(dph, dph, dpdz_out, 0, L, 0))) return rc;
+        }
         return OBL_OK;
     }
 
@@ -344,9 +360,8 @@ template <typename T> struct Ops {
             if ((rc = pad(f[c], (T *)io->big[c], nlev))) return rc;
         }
         if ((rc = press(f[0], f[1], f[2], (const T *)io->divtz_bot, (const T *)io->divtz_top, (T *)io->p,
-                        (T *)io->dp[0], (T *)io->dp[1])))
+                        (T *)io->dp[0], (T *)io->dp[1], (T *)io->dp[2])))
             return rc;
-        if ((rc = dpdz((const T *)io->p, (T *)io->dp[2]))) return rc;
         return project((T *)io->u, (T *)io->v, (T *)io->w, (const T *)io->dp[0], (const T *)io->dp[1],
                        (const T *)io->dp[2]);
     }
@@ -498,29 +513,27 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
     };
     if (!upload(&ctx->d_kx, kx) || !upload(&ctx->d_ky1, ky1) || !upload(&ctx->d_ky2, ky2)) return bad(OBL_ERR_NOMEM);
 
-    // twiddle tables w_N^m = exp(-2 pi i m / N) for every transform length in use
-    for (int n : {ctx->nxt, ctx->nyt, ctx->nxt2, ctx->nyt2}) {
-        if (ctx->tw.count(n)) continue;
-        void *d = nullptr;
-        const size_t b = (ctx->f64 ? sizeof(double2) : sizeof(float2)) * (size_t)n;
-        if (cudaMalloc(&d, b) != cudaSuccess) return bad(OBL_ERR_NOMEM);
-        ctx->tw[n] = d;
-        if (ctx->f64) {
-            std::vector<double2> h(n);
-            for (int m = 0; m < n; ++m) {
-                const double a = -2.0 * kPi * (double)m / (double)n;
-                h[m] = make_double2(std::cos(a), std::sin(a));
+    // plan twiddle tables (FP64 on the host, stored in the storage precision) for the
+    // forward / backward / padded transforms of both horizontal lengths
+    for (int n : {ctx->nxt, ctx->nyt})
+        for (int role = 0; role < 4; ++role) {
+            const int key = 4 * n + role;
+            if (ctx->tw.count(key)) continue;
+            const std::vector<double> h = plan_table(n, role);
+            const size_t m = h.size() / 2;
+            const size_t b = (ctx->f64 ? sizeof(double2) : sizeof(float2)) * (m > 0 ? m : 1);
+            void *d = nullptr;
+            if (cudaMalloc(&d, b) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            ctx->tw[key] = d;
+            if (m == 0) continue;
+            if (ctx->f64) {
+                if (cudaMemcpy(d, h.data(), b, cudaMemcpyHostToDevice) != cudaSuccess) return bad(OBL_ERR_CUDA);
+            } else {
+                std::vector<float2> hf(m);
+                for (size_t i = 0; i < m; ++i) hf[i] = make_float2((float)h[2 * i], (float)h[2 * i + 1]);
+                if (cudaMemcpy(d, hf.data(), b, cudaMemcpyHostToDevice) != cudaSuccess) return bad(OBL_ERR_CUDA);
             }
-            if (cudaMemcpy(d, h.data(), b, cudaMemcpyHostToDevice) != cudaSuccess) return bad(OBL_ERR_CUDA);
-        } else {
-            std::vector<float2> h(n);
-            for (int m = 0; m < n; ++m) {
-                const double a = -2.0 * kPi * (double)m / (double)n;
-                h[m] = make_float2((float)std::cos(a), (float)std::sin(a));
-            }
-            if (cudaMemcpy(d, h.data(), b, cudaMemcpyHostToDevice) != cudaSuccess) return bad(OBL_ERR_CUDA);
         }
-    }
 
     // FP64 islands of the mixed mode: the (0,0) mean mode and every column with
     // k^2 <= fp64_k2_max (weakly diagonally dominant systems)

@@ -1,12 +1,5 @@
-// fft.cuh -- warp-level mixed-radix FFT engine for sm_100a.
-//
-// One warp transforms one "line" (a complex sequence of compile-time length N) that
-// lives in shared memory behind a line accessor.  The transform is a Stockham
-// autosort FFT (natural order in, natural order out): each pass loads the R inputs of
-// every radix-R butterfly into registers, multiplies by the inter-pass twiddles (read
-// from a shared-memory table of w_N^m computed on the host in FP64), runs an
-// in-register DFT_R codelet and stores the R outputs back.  Only __syncwarp() is
-// needed between passes because a line belongs to exactly one warp.
+// fft.cuh -- complex arithmetic helpers and the in-register DFT codelets (radix 2, 3,
+// 4 and the composites 6, 8, 9, 12, 16) used by the Stockham passes of fft2.cuh.
 //
 // Convention (FFTW's, which the reference relies on, SBL/code/002_fft.f90:97-113):
 //   forward  X[k] = sum_j x[j] exp(-2 pi i j k / N)
@@ -215,88 +208,5 @@ template <bool FWD> struct Dft<8, FWD> : DftComp<2, 4, FWD> {};
 template <bool FWD> struct Dft<9, FWD> : DftComp<3, 3, FWD> {};
 template <bool FWD> struct Dft<12, FWD> : DftComp<4, 3, FWD> {};
 template <bool FWD> struct Dft<16, FWD> : DftComp<4, 4, FWD> {};
-
-// ----------------------------------------------------------------------------- plans
-template <int... Rs> struct Plan {};
-
-template <int N> struct PlanFor;
-template <> struct PlanFor<32>  { using type = Plan<2, 4, 4>; };
-template <> struct PlanFor<48>  { using type = Plan<4, 3, 4>; };
-template <> struct PlanFor<64>  { using type = Plan<4, 4, 4>; };
-template <> struct PlanFor<72>  { using type = Plan<4, 3, 6>; };
-template <> struct PlanFor<96>  { using type = Plan<4, 4, 6>; };
-template <> struct PlanFor<128> { using type = Plan<4, 4, 8>; };
-template <> struct PlanFor<144> { using type = Plan<4, 6, 6>; };
-template <> struct PlanFor<192> { using type = Plan<4, 6, 8>; };
-template <> struct PlanFor<256> { using type = Plan<4, 8, 8>; };
-template <> struct PlanFor<288> { using type = Plan<4, 8, 9>; };
-template <> struct PlanFor<384> { using type = Plan<4, 8, 12>; };
-template <> struct PlanFor<512> { using type = Plan<8, 8, 8>; };
-template <> struct PlanFor<576> { using type = Plan<8, 8, 9>; };
-template <> struct PlanFor<768> { using type = Plan<8, 8, 12>; };
-
-// ----------------------------------------------------------------------------- Stockham pass
-// Line accessor concept:  C ld(int i) const;  void st(int i, C v);
-template <int N, int R, int NS, bool FWD, typename C, class Line>
-__device__ __forceinline__ void stockham_pass(Line &L, const C *__restrict__ tw, int lane)
-{
-    constexpr int NB = N / R;
-    constexpr int PER = (NB + 31) / 32;
-    constexpr int TWS = N / (NS * R);   // w_{NS*R}^{rk} = w_N^{r*k*TWS}
-    C v[PER][R];
-#pragma unroll
-    for (int b = 0; b < PER; ++b) {
-        const int j = lane + 32 * b;
-        if ((NB % 32 == 0) || j < NB) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) v[b][r] = L.ld(j + r * NB);
-        }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int b = 0; b < PER; ++b) {
-        const int j = lane + 32 * b;
-        if ((NB % 32 == 0) || j < NB) {
-            const int k = j % NS;
-            if constexpr (NS > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    const C w = tw[r * k * TWS];
-                    v[b][r] = FWD ? cmul(v[b][r], w) : cmulc(v[b][r], w);
-                }
-            }
-            Dft<R, FWD>::run(v[b]);
-            const int base = (j / NS) * NS * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r) L.st(base + r * NS, v[b][r]);
-        }
-    }
-    __syncwarp();
-}
-
-template <int N, int NS, bool FWD, typename C, class Line, int R0, int... Rs>
-__device__ __forceinline__ void fft_passes(Line &L, const C *tw, int lane, Plan<R0, Rs...>)
-{
-    stockham_pass<N, R0, NS, FWD, C>(L, tw, lane);
-    if constexpr (sizeof...(Rs) > 0) fft_passes<N, NS * R0, FWD, C>(L, tw, lane, Plan<Rs...>{});
-}
-
-// In-place transform of the line (length N) by one warp; tw = smem table w_N^m, m < N.
-template <int N, bool FWD, typename C, class Line>
-__device__ __forceinline__ void fft_line(Line &L, const C *tw, int lane)
-{
-    fft_passes<N, 1, FWD, C>(L, tw, lane, typename PlanFor<N>::type{});
-}
-
-// ----------------------------------------------------------------------------- accessors
-// Padded contiguous line in shared memory: element i at base[i + i/8] (breaks the
-// power-of-two store strides of the Stockham passes across banks).
-__host__ __device__ constexpr int line_pad(int n) { return n + n / 8 + 1; }
-
-template <typename C> struct SmemLine {
-    C *base;
-    __device__ __forceinline__ C ld(int i) const { return base[i + (i >> 3)]; }
-    __device__ __forceinline__ void st(int i, C v) { base[i + (i >> 3)] = v; }
-};
 
 } // namespace obl

@@ -4,19 +4,28 @@
 //   rows    (x direction, contiguous):  ddx, x-pad, x-unpad, x r2c, x c2r
 //   columns (y direction, strided):     ddy, y-pad, y-unpad, y c2c forward/backward
 // Real lines are transformed two at a time as one complex line (z = a + i b): every
-// spectral operation used here is a real-to-real linear map that acts on Z[k] and
-// Z[N-k] symmetrically (i*k multipliers with signed k, truncation/zero-extension),
-// so Re(IFFT(op(FFT(z)))) = op(a) and Im(...) = op(b) exactly as the reference's
-// per-line r2c -> op -> c2r computes them (004_derivatives.f90:33-39,
-// 108_01_padd.f90:102-127,163-190).  Columns are staged through a shared-memory tile
-// (the on-GPU replacement of the reference's mpi_alltoall pencil transposes,
-// 203_fftn_mpi.f90:71-371) so global loads and stores stay coalesced along x.
+// spectral operation used here is a real-to-real linear map acting on Z[k] and Z[N-k]
+// symmetrically (i*k multipliers with signed k, truncation / zero extension), so
+// Re(IFFT(op(FFT(z)))) = op(a) and Im(...) = op(b), exactly what the reference's
+// per-line r2c -> op -> c2r computes (004_derivatives.f90:33-39,
+// 108_01_padd.f90:102-127,163-190).
+//
+// Rows are loaded from global memory straight into registers in the layout of the
+// first FFT pass; columns are staged through a shared-memory tile (the on-GPU
+// replacement of the reference's mpi_alltoall pencil transposes,
+// 203_fftn_mpi.f90:71-371) whose padded column doubles as the FFT exchange scratch.
+//
+// Accuracy: before a real line is transformed, its first value is subtracted (exact
+// by Sterbenz's lemma for fields with a large mean such as theta ~ 300 K) and the
+// scale is applied after the subtraction; derivatives ignore the constant, padding
+// adds it back.  FP32 FFT errors then scale with the fluctuations, not with the mean.
 #pragma once
-#include "fft.cuh"
+#include "fft2.cuh"
 
 namespace obl {
 
 enum LineOp : int { OP_DERIV = 0, OP_PAD = 1, OP_UNPAD = 2, OP_FWD = 3, OP_INV = 4 };
+enum PlanRole : int { ROLE_FWD = 0, ROLE_BWD = 1, ROLE_PADFWD = 2, ROLE_PADBWD = 3 };
 
 template <typename T> struct RowArgs {
     const void *src;          // real rows (DERIV/PAD/UNPAD/FWD) or complex rows (INV)
@@ -26,7 +35,7 @@ template <typename T> struct RowArgs {
     long long npairs;         // number of row pairs (rows 2p, 2p+1)
     T scale;                  // multiplies the input at load
     const double *ktab;       // DERIV: k[0..N/2] (the Nyquist entry is 0)
-    const C2<T> *twI, *twO;   // twiddle tables w_N^m for the input / output lengths
+    const C2<T> *twF, *twB;   // plan twiddle tables of the forward / backward transforms
     T pad_scale;              // INV with pad_mode: dst pad columns *= pad_scale
     int pad_mode;
 };
@@ -40,154 +49,262 @@ template <typename T> struct ColArgs {
     int nlev;
     T scale;                         // multiplies the input at load
     const double *ktab;              // DERIV: k[0..N/2]; INV kmul=1: kx per column; kmul=2: ky per row
-    const C2<T> *twI, *twO;
+    const C2<T> *twF, *twB;
     int pad_copy;                    // UNPAD: also write columns 0,1 into ncols, ncols+1
     int zero_nyq;                    // FWD: zero the Nyquist row (203_fftn_mpi.f90:33)
     int kmul;                        // INV: 0 none, 1 multiply by i*kx(col), 2 by i*ky(row)
 };
 
-// ----------------------------------------------------------------------------- accessors
-// Two adjacent real columns (c, c+1) of a real tile with row stride S, viewed as one
-// complex line.
-template <typename T> struct PairLine {
-    T *tile; int S; int c;
-    __device__ __forceinline__ C2<T> ld(int i) const { return mk<T>(tile[i * S + c], tile[i * S + c + 1]); }
-    __device__ __forceinline__ void st(int i, C2<T> v) { tile[i * S + c] = v.x; tile[i * S + c + 1] = v.y; }
+// ----------------------------------------------------------------------------- configuration
+template <int N, int OP> struct LineCfg;
+template <int N> struct LineCfg<N, OP_DERIV> {
+    static constexpr int NI = N, NO = N;
+    using PF = FwdPlan<N>;
+    using PB = BwdPlan<N>;
 };
-template <typename T> struct CplxLine {
-    C2<T> *tile; int S; int c;
-    __device__ __forceinline__ C2<T> ld(int i) const { return tile[i * S + c]; }
-    __device__ __forceinline__ void st(int i, C2<T> v) { tile[i * S + c] = v; }
+template <int N> struct LineCfg<N, OP_PAD> {
+    static constexpr int NI = N, NO = 3 * N / 2;
+    using PF = FwdPlan<N>;
+    using PB = PadBwdPlan<N>;
+};
+template <int N> struct LineCfg<N, OP_UNPAD> {
+    static constexpr int NI = 3 * N / 2, NO = N;
+    using PF = PadFwdPlan<N>;
+    using PB = BwdPlan<N>;
+};
+template <int N> struct LineCfg<N, OP_FWD> : LineCfg<N, OP_DERIV> {};
+template <int N> struct LineCfg<N, OP_INV> : LineCfg<N, OP_DERIV> {};
+
+template <int N, int OP> struct LineDerived {
+    using Cfg = LineCfg<N, OP>;
+    static constexpr int NI = Cfg::NI, NO = Cfg::NO;
+    using PF = typename Cfg::PF;
+    using PB = typename Cfg::PB;
+    static constexpr int llf = LL_<NI, PF>::v, llb = LL_<NO, PB>::v;
+    static constexpr int LL = llf < llb ? llf : llb;
+    static constexpr int LPW = 32 / LL;
+    static constexpr int rf = Regs<NI, LL, PF>::v, rb = Regs<NO, LL, PB>::v;
+    static constexpr int VR = rf > rb ? rf : rb;
+    static constexpr int NM = NI > NO ? NI : NO;
+    static constexpr int TF = tw_size<NI, PF>(), TB = tw_size<NO, PB>();
+    static constexpr int RFL = PlanInfo<PF>::last, RB0 = PlanInfo<PB>::first;
+    static constexpr int RF0 = PlanInfo<PF>::first, RBL = PlanInfo<PB>::last;
 };
 
-// ----------------------------------------------------------------------------- spectral ops
-// z[k] *= i * ks, ks = +k (k <= N/2) or -(N-k); ktab[N/2] = 0 removes the Nyquist mode
-template <typename T, int N, class Line>
-__device__ __forceinline__ void op_deriv(Line &L, const double *ktab, int lane)
+// ----------------------------------------------------------------------------- register ops
+// v in D(R) of length N: v *= i*k_signed (ktab[N/2] = 0 drops the Nyquist mode)
+template <typename T, int N, int R, int LL>
+__device__ __forceinline__ void reg_deriv(C2<T> *v, const double *ktab, int t)
 {
-    for (int k = lane; k < N; k += 32) {
-        const T kk = (k <= N / 2) ? (T)ktab[k] : -(T)ktab[N - k];
-        C2<T> z = L.ld(k);
-        L.st(k, mk<T>(-kk * z.y, kk * z.x));
+    using G = Geo<N, R, LL>;
+#pragma unroll
+    for (int b = 0; b < G::PER; ++b) {
+        const int j = t + LL * b;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int k = j + r * G::NB;
+            const int kc = (G::FULL || j < G::NB) ? k : 0;
+            const T kk = (kc <= N / 2) ? (T)ktab[kc] : -(T)ktab[N - kc];
+            const C2<T> z = v[b * R + r];
+            v[b * R + r] = mk<T>(-kk * z.y, kk * z.x);
+        }
     }
-    __syncwarp();
 }
-// zero-extend the spectrum of length NI to NO = 3 NI / 2, dropping the Nyquist bin
-template <typename T, int NI, int NO, class Line>
-__device__ __forceinline__ void op_pad(Line &L, int lane)
+
+// D(R) of length N  ->  D(3R/2) of length 3N/2, zero-extended, Nyquist bin dropped
+template <typename T, int N, int R, int LL>
+__device__ __forceinline__ void reg_pad(const C2<T> *v, C2<T> *w, int t)
 {
-    for (int m = 1 + lane; m < NI / 2; m += 32) L.st(NO - m, L.ld(NI - m));
-    __syncwarp();
-    for (int k = NI / 2 + lane; k <= NI; k += 32) L.st(k, mk<T>(0, 0));
-    __syncwarp();
+    using G = Geo<N, R, LL>;
+    constexpr int R2 = 3 * R / 2, H = R / 2;
+#pragma unroll
+    for (int b = 0; b < G::PER; ++b) {
+        const int j = t + LL * b;
+#pragma unroll
+        for (int r2 = 0; r2 < R2; ++r2) {
+            C2<T> x = mk<T>(0, 0);
+            if (r2 < H) x = v[b * R + r2];
+            else if (r2 >= R) x = v[b * R + (r2 - H)];
+            if (r2 == R && j == 0) x = mk<T>(0, 0);   // source bin N/2 (Nyquist)
+            w[b * R2 + r2] = x;
+        }
+    }
 }
-// truncate the spectrum of length NI = 3 NO / 2 to NO, zeroing the new Nyquist bin
-template <typename T, int NI, int NO, class Line>
-__device__ __forceinline__ void op_unpad(Line &L, int lane)
+
+// D(3R/2) of length 3N/2  ->  D(R) of length N, truncated, new Nyquist bin zero
+template <typename T, int N, int R, int LL>
+__device__ __forceinline__ void reg_unpad(const C2<T> *w, C2<T> *v, int t)
 {
-    for (int m = 1 + lane; m < NO / 2; m += 32) L.st(NO - m, L.ld(NI - m));
-    __syncwarp();
-    if (lane == 0) L.st(NO / 2, mk<T>(0, 0));
-    __syncwarp();
+    using G = Geo<N, R, LL>;
+    constexpr int R2 = 3 * R / 2, H = R / 2;
+#pragma unroll
+    for (int b = 0; b < G::PER; ++b) {
+        const int j = t + LL * b;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            C2<T> x = (r < H) ? w[b * R2 + r] : w[b * R2 + r + H];
+            if (r == H && j == 0) x = mk<T>(0, 0);     // bin N/2
+            v[b * R + r] = x;
+        }
+    }
 }
 
 // ----------------------------------------------------------------------------- row kernel
-template <typename T, int NI, int NO, int OP>
+template <typename T, int N, int OP>
 __global__ void __launch_bounds__(256) k_rows(RowArgs<T> a)
 {
     using C = C2<T>;
-    constexpr int NM = NI > NO ? NI : NO;
-    constexpr int LP = line_pad(NM);
+    using D = LineDerived<N, OP>;
+    constexpr int NI = D::NI, NO = D::NO, LL = D::LL, LPW = D::LPW, VR = D::VR;
+    constexpr int SL = scratch_len(D::NM);
     extern __shared__ __align__(16) unsigned char smraw[];
-    C *twI = reinterpret_cast<C *>(smraw);
-    C *twO = (NI == NO) ? twI : twI + NI;
-    C *lines = twO + NO;
-    for (int i = threadIdx.x; i < NI; i += blockDim.x) twI[i] = a.twI[i];
-    if (NI != NO)
-        for (int i = threadIdx.x; i < NO; i += blockDim.x) twO[i] = a.twO[i];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + D::TF;
+    C *scr = twB + D::TB;
+    if (OP != OP_INV)
+        for (int i = threadIdx.x; i < D::TF; i += blockDim.x) twF[i] = a.twF[i];
+    if (OP != OP_FWD)
+        for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    SmemLine<C> L{lines + warp * LP};
+    const int g = lane / LL, t = lane % LL;
+    LineScratch<C> sc{scr + (warp * LPW + g) * SL};
 
-    for (long long pr = (long long)blockIdx.x * nw + warp; pr < a.npairs; pr += (long long)gridDim.x * nw) {
-        const long long r0 = 2 * pr;
+    for (long long base = ((long long)blockIdx.x * nw + warp) * LPW; base < a.npairs;
+         base += (long long)gridDim.x * nw * LPW) {
+        const long long pr = base + g;
+        const bool act = pr < a.npairs;
+        const long long r0 = 2 * (act ? pr : 0);
+        C v[VR];
+        T ca = 0, cb = 0;
         if constexpr (OP == OP_INV) {
-            // two Hermitian half spectra A (row r0), B (row r0+1) -> Z = A + iB on all N bins;
-            // Im of the DC and Nyquist bins is ignored, as in FFTW's c2r
-            constexpr int H = NO / 2;
+            // two Hermitian half spectra A (row r0), B (row r0+1) -> Z = A + iB on all N
+            // bins; Im of the DC and Nyquist bins is ignored, as in FFTW's c2r
+            using G = Geo<NO, D::RB0, LL>;
             const C *A = reinterpret_cast<const C *>(a.src) + r0 * a.src_stride;
             const C *B = A + a.src_stride;
-            for (int k = lane; k <= H; k += 32) {
-                C av = A[k], bv = B[k];
-                if (k == 0 || k == H) { av.y = 0; bv.y = 0; }
-                L.st(k, mk<T>(av.x - bv.y, av.y + bv.x));
-                if (k > 0 && k < H) L.st(NO - k, mk<T>(av.x + bv.y, bv.x - av.y));
+#pragma unroll
+            for (int b = 0; b < G::PER; ++b) {
+                const int j = t + LL * b;
+#pragma unroll
+                for (int r = 0; r < D::RB0; ++r) {
+                    const int i = j + r * G::NB;
+                    C z = mk<T>(0, 0);
+                    if (act && (G::FULL || j < G::NB)) {
+                        const bool lo = i <= NO / 2;
+                        const int k = lo ? i : NO - i;
+                        C av = A[k], bv = B[k];
+                        if (k == 0 || k == NO / 2) { av.y = 0; bv.y = 0; }
+                        z = lo ? mk<T>(av.x - bv.y, av.y + bv.x) : mk<T>(av.x + bv.y, bv.x - av.y);
+                    }
+                    v[b * D::RB0 + r] = z;
+                }
             }
         } else {
+            using G = Geo<NI, D::RF0, LL>;
             const T *A = reinterpret_cast<const T *>(a.src) + r0 * a.src_stride;
             const T *B = A + a.src_stride;
-            for (int x = lane; x < NI; x += 32) L.st(x, mk<T>(A[x] * a.scale, B[x] * a.scale));
+            if (act) { ca = A[0]; cb = B[0]; }
+#pragma unroll
+            for (int b = 0; b < G::PER; ++b) {
+                const int j = t + LL * b;
+#pragma unroll
+                for (int r = 0; r < D::RF0; ++r) {
+                    const int i = j + r * G::NB;
+                    C z = mk<T>(0, 0);
+                    if (act && (G::FULL || j < G::NB)) z = mk<T>((A[i] - ca) * a.scale, (B[i] - cb) * a.scale);
+                    v[b * D::RF0 + r] = z;
+                }
+            }
+            fft_regs<NI, typename D::PF, LL, true>(v, sc, twF, t);
         }
-        __syncwarp();
-        if constexpr (OP != OP_INV) fft_line<NI, true, C>(L, twI, lane);
 
         if constexpr (OP == OP_FWD) {
-            // split Z into the half spectra of both rows; zero the x-Nyquist (203_fftn_mpi.f90:25)
-            constexpr int H = NI / 2;
+            // split Z into the half spectra of both rows; zero the x-Nyquist
+            // (203_fftn_mpi.f90:25); the subtracted constants return in the DC bins
+            using G = Geo<NI, D::RFL, LL>;
+#pragma unroll
+            for (int b = 0; b < G::PER; ++b) {
+                const int j = t + LL * b;
+                if (G::FULL || j < G::NB)
+#pragma unroll
+                    for (int r = 0; r < D::RFL; ++r) sc.st(j + r * G::NB, v[b * D::RFL + r]);
+            }
+            __syncwarp();
             C *Ao = reinterpret_cast<C *>(a.dst) + r0 * a.dst_stride;
             C *Bo = Ao + a.dst_stride;
-            for (int k = lane; k <= H; k += 32) {
-                if (k == H) {
-                    Ao[k] = mk<T>(0, 0);
-                    Bo[k] = mk<T>(0, 0);
-                } else {
-                    const C z = L.ld(k), zc = cconj(L.ld(k == 0 ? 0 : NI - k));
+            constexpr int H = NI / 2;
+            for (int k = t; k <= H; k += LL) {
+                C ao = mk<T>(0, 0), bo = mk<T>(0, 0);
+                if (k < H) {
+                    const C z = sc.ld(k), zc = cconj(sc.ld(k == 0 ? 0 : NI - k));
                     const C s = cadd(z, zc), d = csub(z, zc);
-                    Ao[k] = mk<T>((T)0.5 * s.x, (T)0.5 * s.y);
-                    Bo[k] = mk<T>((T)0.5 * d.y, (T)-0.5 * d.x);
+                    ao = mk<T>((T)0.5 * s.x, (T)0.5 * s.y);
+                    bo = mk<T>((T)0.5 * d.y, (T)-0.5 * d.x);
+                    if (k == 0) {
+                        ao.x += ca * a.scale * (T)NI;
+                        bo.x += cb * a.scale * (T)NI;
+                    }
+                }
+                if (act) {
+                    Ao[k] = ao;
+                    Bo[k] = bo;
                 }
             }
             __syncwarp();
         } else {
-            if constexpr (OP == OP_DERIV) op_deriv<T, NI>(L, a.ktab, lane);
-            if constexpr (OP == OP_PAD) op_pad<T, NI, NO>(L, lane);
-            if constexpr (OP == OP_UNPAD) op_unpad<T, NI, NO>(L, lane);
-            fft_line<NO, false, C>(L, twO, lane);
+            C w[VR];
+            C *vb = v;
+            if constexpr (OP == OP_DERIV) reg_deriv<T, N, D::RFL, LL>(v, a.ktab, t);
+            if constexpr (OP == OP_PAD) { reg_pad<T, N, D::RFL, LL>(v, w, t); vb = w; }
+            if constexpr (OP == OP_UNPAD) { reg_unpad<T, N, D::RB0, LL>(v, w, t); vb = w; }
+            fft_regs<NO, typename D::PB, LL, false>(vb, sc, twB, t);
+            using G = Geo<NO, D::RBL, LL>;
             T *A = reinterpret_cast<T *>(a.dst) + r0 * a.dst_stride;
             T *B = A + a.dst_stride;
-            for (int x = lane; x < NO; x += 32) {
-                const C z = L.ld(x);
-                A[x] = z.x;
-                B[x] = z.y;
+            const T addA = (OP == OP_PAD || OP == OP_UNPAD) ? ca : (T)0;
+            const T addB = (OP == OP_PAD || OP == OP_UNPAD) ? cb : (T)0;
+            if (act) {
+#pragma unroll
+                for (int b = 0; b < G::PER; ++b) {
+                    const int j = t + LL * b;
+                    if (G::FULL || j < G::NB)
+#pragma unroll
+                        for (int r = 0; r < D::RBL; ++r) {
+                            const int i = j + r * G::NB;
+                            A[i] = vb[b * D::RBL + r].x + addA;
+                            B[i] = vb[b * D::RBL + r].y + addB;
+                        }
+                }
+                if (OP == OP_INV && a.pad_mode && t < 2) {
+                    A[NO + t] *= a.pad_scale;
+                    B[NO + t] *= a.pad_scale;
+                }
             }
-            if (OP == OP_INV && a.pad_mode && lane < 2) {
-                A[NO + lane] *= a.pad_scale;
-                B[NO + lane] *= a.pad_scale;
-            }
-            __syncwarp();
         }
     }
 }
 
 // ----------------------------------------------------------------------------- column kernel
-template <typename T, bool REAL> struct ColTile {
-    // columns per tile: 128-byte row segments
-    static constexpr int W = REAL ? (int)(128 / sizeof(T)) : (int)(128 / (2 * sizeof(T)));
-    static constexpr int S = W + 1;   // odd row stride (in tile elements)
+template <typename T, bool REAL, int LPW> struct ColTile {
+    static constexpr int LINES = 8 * LPW;                  // lines per CTA (8 warps)
+    static constexpr int W = REAL ? 2 * LINES : LINES;     // tile columns (elements)
+    static constexpr int S = W + 1;                        // odd row stride
 };
 
-template <typename T, int NI, int NO, int OP, bool REAL>
+template <typename T, int N, int OP, bool REAL>
 __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
 {
     using C = C2<T>;
-    using E = typename std::conditional<REAL, T, C>::type;   // tile element
-    constexpr int W = ColTile<T, REAL>::W, S = ColTile<T, REAL>::S;
-    constexpr int NM = NI > NO ? NI : NO;
+    using E = typename std::conditional<REAL, T, C>::type;
+    using D = LineDerived<N, OP>;
+    constexpr int NI = D::NI, NO = D::NO, LL = D::LL, LPW = D::LPW, VR = D::VR;
+    using TT = ColTile<T, REAL, LPW>;
+    constexpr int W = TT::W, S = TT::S;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C *twI = reinterpret_cast<C *>(smraw);
-    C *twO = (NI == NO) ? twI : twI + NI;
-    E *tile = reinterpret_cast<E *>(twO + NO);
-    (void)NM;
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + D::TF;
+    E *tile = reinterpret_cast<E *>(twB + D::TB);
 
     const int z = blockIdx.y;
     const int c0 = blockIdx.x * W;
@@ -195,92 +312,157 @@ __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
     const E *src = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane + c0;
     E *dst = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane + c0;
 
-    for (int i = threadIdx.x; i < NI; i += blockDim.x) twI[i] = a.twI[i];
-    if (NI != NO)
-        for (int i = threadIdx.x; i < NO; i += blockDim.x) twO[i] = a.twO[i];
-
-    // coalesced tile load (rows of W elements), with the optional i*k multiplier
+    if (OP != OP_INV)
+        for (int i = threadIdx.x; i < D::TF; i += blockDim.x) twF[i] = a.twF[i];
+    if (OP != OP_FWD)
+        for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
     for (int idx = threadIdx.x; idx < NI * W; idx += blockDim.x) {
         const int r = idx / W, c = idx - r * W;
         E v;
-        if constexpr (REAL) {
-            v = (c < nc) ? src[(long long)r * a.src_row + c] * a.scale : (T)0;
-        } else {
-            v = (c < nc) ? src[(long long)r * a.src_row + c] : mk<T>(0, 0);
-            if (OP == OP_INV && a.kmul) {
-                const T kk = (T)(a.kmul == 1 ? (c < nc ? a.ktab[c0 + c] : 0.0) : a.ktab[r]);
-                v = mk<T>(-kk * v.y, kk * v.x);
-            }
-            v.x *= a.scale;
-            v.y *= a.scale;
-        }
-        tile[r * S + c] = v;
+        if constexpr (REAL) v = (c < nc) ? src[(long long)r * a.src_row + c] : (T)0;
+        else v = (c < nc) ? src[(long long)r * a.src_row + c] : mk<T>(0, 0);
+        tile[sidx(r) * S + c] = v;
     }
     __syncthreads();
 
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    constexpr int NL = REAL ? W / 2 : W;
-    for (int l = warp; l < NL; l += nw) {
-        const int c = REAL ? 2 * l : l;
-        if (c >= nc) break;
-        auto run = [&](auto &L) {
-            if constexpr (OP != OP_INV) fft_line<NI, true, C>(L, twI, lane);
-            if constexpr (OP == OP_FWD) {
-                if (a.zero_nyq && lane == 0) L.st(NI / 2, mk<T>(0, 0));
-                __syncwarp();
-            } else {
-                if constexpr (OP == OP_DERIV) op_deriv<T, NI>(L, a.ktab, lane);
-                if constexpr (OP == OP_PAD) op_pad<T, NI, NO>(L, lane);
-                if constexpr (OP == OP_UNPAD) op_unpad<T, NI, NO>(L, lane);
-                fft_line<NO, false, C>(L, twO, lane);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / LL, t = lane % LL;
+    const int l = warp * LPW + g;
+    const int c = REAL ? 2 * l : l;
+    const bool act = c < nc;
+    const int cc = act ? c : 0;
+    C v[VR];
+    T cr = 0, ci = 0;
+
+    auto body = [&](auto &acc) {
+        if constexpr (OP != OP_INV) {
+            using G = Geo<NI, D::RF0, LL>;
+            if constexpr (REAL) {
+                const C c0v = acc.ld(0);
+                cr = c0v.x;
+                ci = c0v.y;
             }
-        };
-        if constexpr (REAL) {
-            PairLine<T> L{tile, S, c};
-            run(L);
-        } else {
-            CplxLine<T> L{tile, S, c};
-            run(L);
+#pragma unroll
+            for (int b = 0; b < G::PER; ++b) {
+                const int j = t + LL * b;
+#pragma unroll
+                for (int r = 0; r < D::RF0; ++r) {
+                    C x = mk<T>(0, 0);
+                    if (G::FULL || j < G::NB) {
+                        x = acc.ld(j + r * G::NB);
+                        x.x = (x.x - cr) * a.scale;
+                        x.y = (x.y - ci) * a.scale;
+                    }
+                    v[b * D::RF0 + r] = x;
+                }
+            }
+            __syncwarp();
+            fft_regs<NI, typename D::PF, LL, true>(v, acc, twF, t);
         }
+        if constexpr (OP == OP_FWD) {
+            using G = Geo<NI, D::RFL, LL>;
+#pragma unroll
+            for (int b = 0; b < G::PER; ++b) {
+                const int j = t + LL * b;
+                if (G::FULL || j < G::NB)
+#pragma unroll
+                    for (int r = 0; r < D::RFL; ++r) {
+                        const int i = j + r * G::NB;
+                        C x = v[b * D::RFL + r];
+                        if (a.zero_nyq && i == NI / 2) x = mk<T>(0, 0);
+                        acc.st(i, x);
+                    }
+            }
+        } else {
+            C w[VR];
+            C *vb = v;
+            if constexpr (OP == OP_INV) {
+                using G = Geo<NO, D::RB0, LL>;
+#pragma unroll
+                for (int b = 0; b < G::PER; ++b) {
+                    const int j = t + LL * b;
+#pragma unroll
+                    for (int r = 0; r < D::RB0; ++r) {
+                        const int i = j + r * G::NB;
+                        C x = mk<T>(0, 0);
+                        if (G::FULL || j < G::NB) {
+                            x = acc.ld(i);
+                            if (a.kmul) {
+                                const T kk = (T)(a.kmul == 1 ? a.ktab[c0 + cc] : a.ktab[i]);
+                                x = mk<T>(-kk * x.y, kk * x.x);
+                            }
+                            x.x *= a.scale;
+                            x.y *= a.scale;
+                        }
+                        v[b * D::RB0 + r] = x;
+                    }
+                }
+                __syncwarp();
+            }
+            if constexpr (OP == OP_DERIV) reg_deriv<T, N, D::RFL, LL>(v, a.ktab, t);
+            if constexpr (OP == OP_PAD) { reg_pad<T, N, D::RFL, LL>(v, w, t); vb = w; }
+            if constexpr (OP == OP_UNPAD) { reg_unpad<T, N, D::RB0, LL>(v, w, t); vb = w; }
+            fft_regs<NO, typename D::PB, LL, false>(vb, acc, twB, t);
+            using G = Geo<NO, D::RBL, LL>;
+            const T ar = (OP == OP_PAD || OP == OP_UNPAD) ? cr : (T)0;
+            const T ai = (OP == OP_PAD || OP == OP_UNPAD) ? ci : (T)0;
+#pragma unroll
+            for (int b = 0; b < G::PER; ++b) {
+                const int j = t + LL * b;
+                if (G::FULL || j < G::NB)
+#pragma unroll
+                    for (int r = 0; r < D::RBL; ++r) {
+                        C x = vb[b * D::RBL + r];
+                        x.x += ar;
+                        x.y += ai;
+                        acc.st(j + r * G::NB, x);
+                    }
+            }
+        }
+    };
+    if constexpr (REAL) {
+        TilePair<T> acc{tile, S, cc, act};
+        body(acc);
+    } else {
+        TileCol<C> acc{tile, S, cc, act};
+        body(acc);
     }
     __syncthreads();
 
     for (int idx = threadIdx.x; idx < NO * W; idx += blockDim.x) {
-        const int r = idx / W, c = idx - r * W;
-        if (c < nc) dst[(long long)r * a.dst_row + c] = tile[r * S + c];
+        const int r = idx / W, cx = idx - r * W;
+        if (cx < nc) dst[(long long)r * a.dst_row + cx] = tile[sidx(r) * S + cx];
     }
     if constexpr (OP == OP_UNPAD && REAL) {
         // var(nxt+1:ldx,:) = var(1:2,:) (108_01_padd.f90:195)
         if (a.pad_copy && c0 == 0)
             for (int r = threadIdx.x; r < NO; r += blockDim.x) {
                 E *d = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane + (long long)r * a.dst_row;
-                d[a.ncols] = tile[r * S + 0];
-                d[a.ncols + 1] = tile[r * S + 1];
+                d[a.ncols] = tile[sidx(r) * S + 0];
+                d[a.ncols + 1] = tile[sidx(r) * S + 1];
             }
     }
 }
 
 // ----------------------------------------------------------------------------- launchers
-template <typename T, int NI, int NO, int OP>
-inline size_t rows_smem()
+template <typename T, int N, int OP> inline size_t rows_smem()
 {
-    constexpr int NM = NI > NO ? NI : NO;
-    return sizeof(C2<T>) * ((NI == NO ? NI : NI + NO) + 8 * line_pad(NM));
+    using D = LineDerived<N, OP>;
+    return sizeof(C2<T>) * ((size_t)D::TF + D::TB + (size_t)8 * D::LPW * scratch_len(D::NM));
 }
-template <typename T, int NI, int NO, int OP, bool REAL>
-inline size_t cols_smem()
+template <typename T, int N, int OP, bool REAL> inline size_t cols_smem()
 {
-    constexpr int NM = NI > NO ? NI : NO;
+    using D = LineDerived<N, OP>;
     using E = typename std::conditional<REAL, T, C2<T>>::type;
-    return sizeof(C2<T>) * (NI + NO) + sizeof(E) * (size_t)NM * ColTile<T, REAL>::S;
+    using TT = ColTile<T, REAL, D::LPW>;
+    return sizeof(C2<T>) * ((size_t)D::TF + D::TB) + sizeof(E) * (size_t)tile_rows(D::NM) * TT::S;
 }
 
-template <typename T, int NI, int NO, int OP>
-cudaError_t launch_rows_t(const RowArgs<T> &a, cudaStream_t s)
+template <typename T, int N, int OP> cudaError_t launch_rows_t(const RowArgs<T> &a, cudaStream_t s)
 {
     static int grid_cap = 0;
-    const size_t sm = rows_smem<T, NI, NO, OP>();
-    auto kern = k_rows<T, NI, NO, OP>;
+    const size_t sm = rows_smem<T, N, OP>();
+    auto kern = k_rows<T, N, OP>;
     if (!grid_cap) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
@@ -290,25 +472,26 @@ cudaError_t launch_rows_t(const RowArgs<T> &a, cudaStream_t s)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
         grid_cap = nsm * (per > 0 ? per : 1);
     }
-    long long want = (a.npairs + 7) / 8;
+    constexpr int LPW = LineDerived<N, OP>::LPW;
+    const long long per_cta = 8LL * LPW;
+    long long want = (a.npairs + per_cta - 1) / per_cta;
     int grid = (int)(want < grid_cap ? want : grid_cap);
     if (grid < 1) return cudaSuccess;
     kern<<<grid, 256, sm, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename T, int NI, int NO, int OP, bool REAL>
-cudaError_t launch_cols_t(const ColArgs<T> &a, cudaStream_t s)
+template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const ColArgs<T> &a, cudaStream_t s)
 {
     static bool init = false;
-    const size_t sm = cols_smem<T, NI, NO, OP, REAL>();
-    auto kern = k_cols<T, NI, NO, OP, REAL>;
+    const size_t sm = cols_smem<T, N, OP, REAL>();
+    auto kern = k_cols<T, N, OP, REAL>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         init = true;
     }
-    constexpr int W = ColTile<T, REAL>::W;
+    constexpr int W = ColTile<T, REAL, LineDerived<N, OP>::LPW>::W;
     dim3 grid((a.ncols + W - 1) / W, a.nlev);
     if (grid.x < 1 || grid.y < 1) return cudaSuccess;
     kern<<<grid, 256, sm, s>>>(a);
@@ -319,5 +502,7 @@ cudaError_t launch_cols_t(const ColArgs<T> &a, cudaStream_t s)
 template <typename T> cudaError_t launch_rows(int op, int n, const RowArgs<T> &a, cudaStream_t s);
 template <typename T> cudaError_t launch_cols(int op, bool real, int n, const ColArgs<T> &a, cudaStream_t s);
 bool line_length_supported(int n);
+// twiddle table (interleaved re,im in FP64) of the plan with the given role for base length n
+std::vector<double> plan_table(int n, int role);
 
 } // namespace obl

@@ -40,6 +40,8 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
     // Nyquist columns: p_hat = 0 at every level (:303-305, and the caller's zero fill)
     if (ix == a.lhx - 1 || iy == a.nyt / 2) {
         for (int z = 0; z <= L; ++z) ph[S * z] = mk<TS>(0, 0);
+        if (a.dph)
+            for (int z = 1; z <= L; ++z) a.dph[q + S * z] = mk<TS>(0, 0);
         return;
     }
     const double kxd = a.kx[ix], kyd = a.ky[iy];
@@ -106,14 +108,19 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
     // ---- back substitution ----
     CC pn = a.neumann_top ? dprev : mk<TC>(0, 0);   // p_hat(nz-1): solved row / forced 0
     ph[S * L] = mk<TS>((TS)pn.x, (TS)pn.y);
+    C2<TS> *dph = a.dph ? a.dph + q : nullptr;
     for (int iz = L - 1; iz >= 1; --iz) {
         const CC d = ld_d(iz);
         const TC cp = ld_c(iz);
-        pn = mk<TC>(d.x - cp * pn.x, d.y - cp * pn.y);
-        ph[S * iz] = mk<TS>((TS)pn.x, (TS)pn.y);
+        const CC p = mk<TC>(d.x - cp * pn.x, d.y - cp * pn.y);
+        if (dph) dph[S * (iz + 1)] = mk<TS>((TS)((pn.x - p.x) / dz), (TS)((pn.y - p.y) / dz));
+        ph[S * iz] = mk<TS>((TS)p.x, (TS)p.y);
+        pn = p;
     }
     // Neumann ghost level below the wall (:313-315)
-    ph[0] = mk<TS>((TS)(pn.x - dz * hz0.x), (TS)(pn.y - dz * hz0.y));
+    const CC p0 = mk<TC>(pn.x - dz * hz0.x, pn.y - dz * hz0.y);
+    ph[0] = mk<TS>((TS)p0.x, (TS)p0.y);
+    if (dph) dph[S] = mk<TS>((TS)((pn.x - p0.x) / dz), (TS)((pn.y - p0.y) / dz));
 }
 
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e)

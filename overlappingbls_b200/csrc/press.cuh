@@ -8,6 +8,8 @@ namespace obl {
 template <typename T> struct TdmaArgs {
     const C2<T> *Hx, *Hy, *Hz;  // spectral planes (lhx, nyt) of levels 0..nz (Hx,Hy use 1..L)
     C2<T> *phat;                // out: levels 0..L
+    C2<T> *dph;                 // optional out: (p_hat(z) - p_hat(z-1))/dz at levels 1..L,
+                                // formed in the solve's precision (the spectrum of dpdz)
     T *cscr;                    // bulk scratch: modified upper band c'(1..L), (S, L)
     const double *kx;           // kx(lhx), Nyquist entry 0       (002_fft.f90:131-137)
     const double *ky;           // ky_2d row (nyt), Nyquist row 0 (002_fft.f90:147,161-165)
