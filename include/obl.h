@@ -128,6 +128,25 @@ int obl_zero_unpadding(obl_ctx *ctx, const double *var_big, double *var, int nle
 int obl_zero_padding_dev(obl_ctx *ctx, const void *var, void *var_big, int nlev);
 int obl_zero_unpadding_dev(obl_ctx *ctx, const void *var_big, void *var, int nlev);
 
+/* ---- zero_padding that allocates nothing (no counterpart in the reference) ----
+   For callers that cannot allocate device memory when they call: code running while a
+   CUDA graph is being captured, or an application that reserves all device memory at
+   start-up and forbids allocation afterwards.  Same arguments and result as
+   obl_zero_padding_dev, but the intermediate x-padded plane lives in a static device
+   array of OBL_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
+   the process exits; the call itself performs no cudaMalloc/cudaFree.
+   - Sizes: es * nxt2 * nyt * nlev must fit in OBL_NOALLOC_SCRATCH_BYTES (es = 8 for
+     OBL_PREC_F64, 4 otherwise); larger requests return OBL_ERR_ARG with an explanation
+     in obl_last_error (pass fewer levels per call).
+   - The first call on a device looks up the array's device address
+     (cudaGetSymbolAddress) with that device current; make that first call before any
+     stream capture.
+   - All calls share the one array: calls that overlap on the GPU (different streams or
+     contexts without ordering) race on it.  Every element of the scratch is rewritten
+     before it is read, so nothing needs clearing between calls. */
+#define OBL_NOALLOC_SCRATCH_BYTES (8u << 20)
+int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void *var_big, int nlev);
+
 /* ---- filter_data (006_test_filter.f90:82-105): in place on (ldx, nyt, nlev) ---- */
 int obl_filter_data(obl_ctx *ctx, double *f, int nlev);
 int obl_filter_data_dev(obl_ctx *ctx, void *f, int nlev);

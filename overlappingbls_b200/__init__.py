@@ -36,6 +36,7 @@ EXPORTS = [
     "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
     "obl_zero_padding", "obl_zero_unpadding", "obl_zero_padding_dev", "obl_zero_unpadding_dev",
+    "obl_zero_padding_noalloc_dev",
     "obl_filter_data", "obl_filter_data_dev",
     "obl_press_stag_array", "obl_press_stag_array_dev",
     "obl_dpdz", "obl_dpdz_dev", "obl_project", "obl_project_dev",
@@ -105,6 +106,7 @@ def load_library(path=LIB_PATH):
         "obl_fftn_dev": [ctx, P, P, I], "obl_ifftn_dev": [ctx, P, P, I],
         "obl_zero_padding": [ctx, P, P, I], "obl_zero_unpadding": [ctx, P, P, I],
         "obl_zero_padding_dev": [ctx, P, P, I], "obl_zero_unpadding_dev": [ctx, P, P, I],
+        "obl_zero_padding_noalloc_dev": [ctx, P, P, I],
         "obl_filter_data": [ctx, P, I], "obl_filter_data_dev": [ctx, P, I],
         "obl_press_stag_array": [ctx, P, P, P, P, P, P, P, P],
         "obl_press_stag_array_dev": [ctx, P, P, P, P, P, P, P, P],
@@ -294,6 +296,12 @@ class Context:
 
     def zero_padding_dev(self, var, var_big, nlev):
         self._check(self._lib.obl_zero_padding_dev(self._h, var, var_big, nlev), "zero_padding_dev")
+
+    def zero_padding_noalloc_dev(self, var, var_big, nlev):
+        """zero_padding into a static device scratch: the call allocates nothing (for
+        callers that may not allocate, e.g. during CUDA graph capture)."""
+        self._check(self._lib.obl_zero_padding_noalloc_dev(self._h, var, var_big, nlev),
+                    "zero_padding_noalloc_dev")
 
     def zero_unpadding_dev(self, var_big, var, nlev):
         self._check(self._lib.obl_zero_unpadding_dev(self._h, var_big, var, nlev), "zero_unpadding_dev")

@@ -181,6 +181,17 @@ template <typename T> struct Ops {
         auto ca = colargs(xb, nx2, (long long)nx2 * ny, big, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny, OP_PAD, ny);
         return cols(OP_PAD, true, ny, ca, "pad_cols");
     }
+    // zero_padding through a caller-independent scratch plane xb (nxt2*nyt*nlev reals)
+    // instead of the context's allocated buffer; used by obl_zero_padding_noalloc_dev
+    int pad_with_scratch(const T *var, T *big, T *xb, int nlev)
+    {
+        const int nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        auto ra = rowargs(var, ctx->ldx, xb, nx2, (long long)ny * nlev, 1.0 / nx, OP_PAD, nx);
+        int rc = rows(OP_PAD, nx, ra, "pad_rows_noalloc");
+        if (rc) return rc;
+        auto ca = colargs(xb, nx2, (long long)nx2 * ny, big, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny, OP_PAD, ny);
+        return cols(OP_PAD, true, ny, ca, "pad_cols_noalloc");
+    }
     int unpad(const T *big, T *var, int nlev)
     {
         const int nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
@@ -935,3 +946,57 @@ int obl_step_f32(obl_ctx *ctx, const obl_step_io *io)
 }
 
 } // extern "C"
+
+// ============================================================================= no-allocation variant
+// Some callers cannot allocate device memory at call time: code that runs while a CUDA
+// graph is being captured, or an application that reserves all device memory up front
+// and forbids allocation afterwards.  For them zero_padding has one variant whose
+// intermediate x-padded plane lives in a fixed-size static device array instead of a
+// buffer that the context allocates on first use.  The array is part of the module
+// image, so every GPU that loads this library holds OBL_NOALLOC_SCRATCH_BYTES until the
+// process exits.
+namespace {
+constexpr size_t kNoAllocBytes = OBL_NOALLOC_SCRATCH_BYTES;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device with that device
+// current.  In host code the array's name is only a host-side stand-in, never a device
+// address, so kernels receive this looked-up pointer.
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64];
+
+int noalloc_scratch(obl_ctx *ctx, void **out)
+{
+    if (ctx->dev < 0 || ctx->dev >= 64)
+        return fail(ctx, OBL_ERR_ARG, "zero_padding_noalloc: device ordinal beyond the scratch table");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[ctx->dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        if (!p) return fail(ctx, OBL_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) returned NULL");
+        g_noalloc_ptr[ctx->dev] = p;
+    }
+    *out = g_noalloc_ptr[ctx->dev];
+    return OBL_OK;
+}
+} // namespace
+
+extern "C" int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void *var_big, int nlev)
+{
+    if (!ctx || !var || !var_big || !nlev_ok(ctx, nlev)) return OBL_ERR_ARG;
+    const size_t need = ctx->es() * (size_t)ctx->nxt2 * (size_t)ctx->nyt * (size_t)nlev;
+    if (need > kNoAllocBytes)
+        return fail(ctx, OBL_ERR_ARG,
+                    "zero_padding_noalloc: " + std::to_string(nlev) + " level(s) need " + std::to_string(need) +
+                        " bytes of scratch but the static scratch holds " + std::to_string(kNoAllocBytes) +
+                        " bytes; pass fewer levels per call");
+    if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice");
+    void *xb = nullptr;
+    const int rc = noalloc_scratch(ctx, &xb);
+    if (rc) return rc;
+    return dispatchT(ctx, [&](auto &o) -> int {
+        using T = typename std::remove_reference<decltype(o)>::type::Tt;
+        return o.pad_with_scratch((const T *)var, (T *)var_big, (T *)xb, nlev);
+    });
+}
