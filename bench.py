@@ -138,6 +138,9 @@ def run_ours(args, rank, local, world):
     def make_ctx(prec):
         c = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", device=local, **fields.DOMAIN)
         c.set_stream(stream.cuda_stream)
+        for kv in args.param:
+            k, v = kv.split("=")
+            c.set_param(k, int(v))
         return c
 
     def dev_set(ctx, dtype):
@@ -391,6 +394,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--param", action="append", default=[],
+                    help="execution tuning name=value passed to obl_set_param (e.g. fused=0)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, local, world = env_rank()

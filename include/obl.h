@@ -97,6 +97,12 @@ long long obl_launch_count(const obl_ctx *ctx);
    {"kernel": [launches, total_ms], ...} (synchronizes; clears the records) */
 int obl_timing_enable(obl_ctx *ctx, int on);
 int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
+/* execution tuning (results do not depend on it):
+     "fused"             1 = cluster-fused plane kernels in obl_step (square grids), 0 = line kernels
+     "fwd_clusters"      clusters of the fused forward kernel (0 = as many as can be resident)
+     "fwd_cluster_size"  CTAs per cluster (1..16; above 8 needs non-portable cluster support) */
+int obl_set_param(obl_ctx *ctx, const char *name, long long value);
+int obl_get_param(obl_ctx *ctx, const char *name, long long *value);
 
 /* ---- spectral derivatives: ddx / ddy (004_derivatives.f90:18-41, 45-81) ----
    fields (ldx, nyt, nlev) (the reference passes nlev = nz+1); x < nxt written. */

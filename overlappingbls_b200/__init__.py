@@ -32,6 +32,7 @@ TOP_BC = {"single": 0, "neumann": 1}
 EXPORTS = [
     "obl_ctx_create", "obl_ctx_destroy", "obl_ctx_info", "obl_set_stream", "obl_synchronize",
     "obl_last_error", "obl_launch_count", "obl_timing_enable", "obl_timing_report",
+    "obl_set_param", "obl_get_param",
     "obl_ddx", "obl_ddy", "obl_ddx_dev", "obl_ddy_dev",
     "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
@@ -98,6 +99,8 @@ def load_library(path=LIB_PATH):
         "obl_set_stream": [ctx, P], "obl_synchronize": [ctx],
         "obl_last_error": [ctx, ctypes.c_char_p, ctypes.c_size_t],
         "obl_timing_enable": [ctx, I], "obl_timing_report": [ctx, ctypes.c_char_p, ctypes.c_size_t],
+        "obl_set_param": [ctx, ctypes.c_char_p, ctypes.c_longlong],
+        "obl_get_param": [ctx, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)],
         "obl_ddx": [ctx, P, P, I], "obl_ddy": [ctx, P, P, I],
         "obl_ddx_dev": [ctx, P, P, I], "obl_ddy_dev": [ctx, P, P, I],
         "obl_ddz_uv": [ctx, P, P], "obl_ddz_w": [ctx, P, P],
@@ -195,6 +198,14 @@ class Context:
 
     def launch_count(self):
         return int(self._lib.obl_launch_count(self._h))
+
+    def set_param(self, name, value):
+        self._check(self._lib.obl_set_param(self._h, name.encode(), int(value)), "obl_set_param")
+
+    def get_param(self, name):
+        v = ctypes.c_longlong()
+        self._check(self._lib.obl_get_param(self._h, name.encode(), ctypes.byref(v)), "obl_get_param")
+        return v.value
 
     def timing(self, on=True):
         self._check(self._lib.obl_timing_enable(self._h, 1 if on else 0), "obl_timing_enable")

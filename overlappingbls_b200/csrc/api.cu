@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "lines.cuh"
 #include "press.cuh"
+#include "fused.cuh"
 
 using namespace obl;
 
@@ -51,6 +52,11 @@ struct obl_ctx {
     DevBuf cscr;               // c' scratch
     DevBuf isl_c, isl_d;
     DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
+    DevBuf fscr;               // cluster scratch slots of the fused forward kernel
+    // tuning parameters (obl_set_param)
+    long long param_fused = 1;          // use the cluster-fused kernels in obl_step
+    long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
+    long long param_fwd_csize = 8;      // CTAs per cluster
     std::vector<DevBuf> stage; // host-variant staging (storage type)
     std::vector<DevBuf> stage64;
 
@@ -246,8 +252,10 @@ template <typename T> struct Ops {
     // dpdz (optional): also return dpdz = ifftn((p_hat(z) - p_hat(z-1))/dz), the
     // spectral form of the flosol difference (103_flosol.f90:174-175), whose
     // z-difference is taken inside the solve in its own precision
+    // rhs_ready: H_x, H_y, H_z at levels 1..L were already produced (by the fused
+    // forward kernel); only the boundary planes H_z(0), H_z(nz) are transformed here.
     int press(const T *u, const T *v, const T *w, const T *dbot, const T *dtop, T *p, T *dpdx, T *dpdy,
-              T *dpdz_out = nullptr)
+              T *dpdz_out = nullptr, bool rhs_ready = false)
     {
         const long long S = ctx->sp();
         const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
@@ -265,7 +273,7 @@ template <typename T> struct Ops {
         // x r2c of levels 1..L of u, v, w straight into the spectral buffers
         const T *src[3] = {u, v, w};
         C2<T> *dst[3] = {Hx, Hy, Hz};
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < 3 && !rhs_ready; ++c) {
             auto ra = rowargs(src[c] + pl, ldx, dst[c] + S, lhx, (long long)ny * L, sc, OP_FWD, nx);
             if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
         }
@@ -283,7 +291,7 @@ template <typename T> struct Ops {
             CK(cudaMemsetAsync(Hz + S * (L + 1), 0, sizeof(C2<T>) * S, s()));
         }
         // y c2c (in place), y-Nyquist zeroed
-        {
+        if (!rhs_ready) {
             auto ca = colargs(Hx + S, lhx, S, Hx + S, lhx, S, lhx, L, 1.0, OP_FWD, ny);
             ca.zero_nyq = 1;
             if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
@@ -292,6 +300,12 @@ template <typename T> struct Ops {
             ca.src = ca.dst = Hz;
             ca.nlev = L + 2;
             if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
+        } else {
+            for (int zb : {0, L + 1}) {
+                auto ca = colargs(Hz + S * zb, lhx, S, Hz + S * zb, lhx, S, lhx, 1, 1.0, OP_FWD, ny);
+                ca.zero_nyq = 1;
+                if ((rc = cols(OP_FWD, false, ny, ca, "press_bnd_cols"))) return rc;
+            }
         }
         // tridiagonal solve per (kx,ky) column
         TdmaArgs<T> ta{};
@@ -360,11 +374,61 @@ template <typename T> struct Ops {
     }
 
     // ---- the fused step ----
+    // cluster-fused forward pass over all (field, level) planes: ddx, ddy, zero_padding of
+    // u, v, w, theta and the RHS spectra H_x, H_y, H_z of levels 1..L
+    int fwd_fused(const obl_step_io *io)
+    {
+        const long long S = ctx->sp();
+        const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
+        int rc;
+        for (int i = 0; i < 5; ++i)
+            if ((rc = ensure(ctx, ctx->spec[i], sb))) return rc;
+        const int n = ctx->nxt, csize = (int)ctx->param_fwd_csize;
+        int ncl = (int)ctx->param_fwd_clusters;
+        const int maxc = FwdFusedLaunch<T>::max_clusters(n, csize);
+        if (maxc <= 0) return fail(ctx, OBL_ERR_UNSUPPORTED, "fused forward kernel cannot be resident");
+        if (ncl <= 0 || ncl > maxc) ncl = maxc;
+        const int nitems = 4 * (ctx->nz + 1);
+        if (ncl > nitems) ncl = nitems;
+        const size_t slot = FwdFusedLaunch<T>::slot_bytes(n);
+        if ((rc = ensure(ctx, ctx->fscr, slot * (size_t)ncl))) return rc;
+        FwdFusedArgs<T> a{};
+        for (int c = 0; c < 4; ++c) {
+            a.f[c] = c == 0 ? (const T *)io->u : c == 1 ? (const T *)io->v : c == 2 ? (const T *)io->w
+                                                                             : (const T *)io->theta;
+            a.big[c] = (T *)io->big[c];
+        }
+        for (int i = 0; i < 8; ++i) a.d[i] = (T *)io->d[i];
+        for (int c = 0; c < 3; ++c) a.H[c] = (C2<T> *)ctx->spec[c].p;
+        a.scr = (unsigned char *)ctx->fscr.p;
+        a.slot_bytes = (long long)slot;
+        a.ldx = ctx->ldx;
+        a.nlev = ctx->nz + 1;
+        a.L = ctx->L;
+        a.nfields = 4;
+        a.sc_press = ((1.0 / ((double)ctx->nxt * ctx->nyt)) / kTadv1) * (1.0 / ctx->dt_nd);
+        a.kx = ctx->d_kx;
+        a.ky = ctx->d_ky1;
+        a.twF = twt<T>(ctx, n, ROLE_FWD);
+        a.twB = twt<T>(ctx, n, ROLE_BWD);
+        a.twPB = twt<T>(ctx, n, ROLE_PADBWD);
+        LaunchScope ls(ctx->rec, "fwd_fused", s());
+        return chk(FwdFusedLaunch<T>::run(n, a, ncl, csize, s()), "fwd_fused");
+    }
+
     int step(const obl_step_io *io)
     {
         const int nlev = ctx->nz + 1;
         const T *f[4] = {(const T *)io->u, (const T *)io->v, (const T *)io->w, (const T *)io->theta};
         int rc;
+        if (ctx->param_fused && ctx->nxt == ctx->nyt) {
+            if ((rc = fwd_fused(io))) return rc;
+            if ((rc = press(f[0], f[1], f[2], (const T *)io->divtz_bot, (const T *)io->divtz_top, (T *)io->p,
+                            (T *)io->dp[0], (T *)io->dp[1], (T *)io->dp[2], true)))
+                return rc;
+            return project((T *)io->u, (T *)io->v, (T *)io->w, (const T *)io->dp[0], (const T *)io->dp[1],
+                           (const T *)io->dp[2]);
+        }
         for (int c = 0; c < 4; ++c) {
             if ((rc = ddx((T *)io->d[2 * c], f[c], nlev))) return rc;
             if ((rc = ddy((T *)io->d[2 * c + 1], f[c], nlev))) return rc;
@@ -591,6 +655,7 @@ int obl_ctx_destroy(obl_ctx *ctx)
     cudaFree(ctx->isl_c.p);
     cudaFree(ctx->isl_d.p);
     cudaFree(ctx->tmp.p);
+    cudaFree(ctx->fscr.p);
     for (auto &b : ctx->stage) cudaFree(b.p);
     for (auto &b : ctx->stage64) cudaFree(b.p);
     delete ctx;
@@ -633,6 +698,34 @@ int obl_last_error(const obl_ctx *ctx, char *buf, size_t n)
 }
 
 long long obl_launch_count(const obl_ctx *ctx) { return ctx ? ctx->rec.launches : -1; }
+
+static long long *param_slot(obl_ctx *ctx, const char *name)
+{
+    if (!std::strcmp(name, "fused")) return &ctx->param_fused;
+    if (!std::strcmp(name, "fwd_clusters")) return &ctx->param_fwd_clusters;
+    if (!std::strcmp(name, "fwd_cluster_size")) return &ctx->param_fwd_csize;
+    return nullptr;
+}
+
+int obl_set_param(obl_ctx *ctx, const char *name, long long value)
+{
+    if (!ctx || !name) return OBL_ERR_ARG;
+    long long *p = param_slot(ctx, name);
+    if (!p) return fail(ctx, OBL_ERR_ARG, std::string("unknown parameter ") + name);
+    if (!std::strcmp(name, "fwd_cluster_size") && (value < 1 || value > 16))
+        return fail(ctx, OBL_ERR_ARG, "fwd_cluster_size must be 1..16");
+    *p = value;
+    return OBL_OK;
+}
+
+int obl_get_param(obl_ctx *ctx, const char *name, long long *value)
+{
+    if (!ctx || !name || !value) return OBL_ERR_ARG;
+    long long *p = param_slot(ctx, name);
+    if (!p) return fail(ctx, OBL_ERR_ARG, std::string("unknown parameter ") + name);
+    *value = *p;
+    return OBL_OK;
+}
 
 int obl_timing_enable(obl_ctx *ctx, int on)
 {

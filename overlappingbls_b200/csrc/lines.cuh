@@ -20,6 +20,8 @@
 // scale is applied after the subtraction; derivatives ignore the constant, padding
 // adds it back.  FP32 FFT errors then scale with the fluctuations, not with the mean.
 #pragma once
+#include <vector>
+
 #include "fft2.cuh"
 
 namespace obl {
@@ -53,6 +55,8 @@ template <typename T> struct ColArgs {
     int pad_copy;                    // UNPAD: also write columns 0,1 into ncols, ncols+1
     int zero_nyq;                    // FWD: zero the Nyquist row (203_fftn_mpi.f90:33)
     int kmul;                        // INV: 0 none, 1 multiply by i*kx(col), 2 by i*ky(row)
+    int ldcg;                        // load the source with ld.global.cg (L2 only): the source
+                                     // was written by other CTAs since this SM last read it
 };
 
 // ----------------------------------------------------------------------------- configuration
@@ -150,28 +154,31 @@ __device__ __forceinline__ void reg_unpad(const C2<T> *w, C2<T> *v, int t)
 }
 
 // ----------------------------------------------------------------------------- row kernel
+// copy the plan twiddle tables an op needs into shared memory (caller syncs)
 template <typename T, int N, int OP>
-__global__ void __launch_bounds__(256) k_rows(RowArgs<T> a)
+__device__ __forceinline__ void load_tables(const C2<T> *gF, const C2<T> *gB, C2<T> *sF, C2<T> *sB)
+{
+    using D = LineDerived<N, OP>;
+    if (OP != OP_INV)
+        for (int i = threadIdx.x; i < D::TF; i += blockDim.x) sF[i] = gF[i];
+    if (OP != OP_FWD)
+        for (int i = threadIdx.x; i < D::TB; i += blockDim.x) sB[i] = gB[i];
+}
+
+// One warp processes the LPW row pairs base .. base+LPW-1 (pairs at or beyond a.npairs
+// idle).  twF/twB: the plan twiddle tables in shared memory; scr_warp: the warp's
+// scratch lines (LPW * scratch_len(NM) complex).
+template <typename T, int N, int OP>
+__device__ __forceinline__ void row_unit(const RowArgs<T> &a, long long base, const C2<T> *twF,
+                                         const C2<T> *twB, C2<T> *scr_warp, int lane)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP>;
-    constexpr int NI = D::NI, NO = D::NO, LL = D::LL, LPW = D::LPW, VR = D::VR;
+    constexpr int NI = D::NI, NO = D::NO, LL = D::LL, VR = D::VR;
     constexpr int SL = scratch_len(D::NM);
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twF = reinterpret_cast<C *>(smraw);
-    C *twB = twF + D::TF;
-    C *scr = twB + D::TB;
-    if (OP != OP_INV)
-        for (int i = threadIdx.x; i < D::TF; i += blockDim.x) twF[i] = a.twF[i];
-    if (OP != OP_FWD)
-        for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int g = lane / LL, t = lane % LL;
-    LineScratch<C> sc{scr + (warp * LPW + g) * SL};
-
-    for (long long base = ((long long)blockIdx.x * nw + warp) * LPW; base < a.npairs;
-         base += (long long)gridDim.x * nw * LPW) {
+    LineScratch<C> sc{scr_warp + g * SL};
+    {
         const long long pr = base + g;
         const bool act = pr < a.npairs;
         const long long r0 = 2 * (act ? pr : 0);
@@ -285,6 +292,23 @@ __global__ void __launch_bounds__(256) k_rows(RowArgs<T> a)
     }
 }
 
+template <typename T, int N, int OP>
+__global__ void __launch_bounds__(256) k_rows(RowArgs<T> a)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + D::TF;
+    C *scr = twB + D::TB;
+    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (long long base = ((long long)blockIdx.x * nw + warp) * D::LPW; base < a.npairs;
+         base += (long long)gridDim.x * nw * D::LPW)
+        row_unit<T, N, OP>(a, base, twF, twB, scr + warp * D::LPW * scratch_len(D::NM), lane);
+}
+
 // ----------------------------------------------------------------------------- column kernel
 template <typename T, bool REAL, int LPW> struct ColTile {
     static constexpr int LINES = 8 * LPW;                  // lines per CTA (8 warps)
@@ -292,8 +316,13 @@ template <typename T, bool REAL, int LPW> struct ColTile {
     static constexpr int S = W + 1;                        // odd row stride
 };
 
+// The whole CTA processes column tile tx of plane z: coalesced tile load, one line per
+// LL lanes through forward -> op -> backward in registers (the tile column is the
+// exchange scratch), coalesced store.  Contains __syncthreads(): call uniformly.
 template <typename T, int N, int OP, bool REAL>
-__global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
+__device__ __forceinline__ void col_unit(const ColArgs<T> &a, int z, int tx, const C2<T> *twF,
+                                         const C2<T> *twB,
+                                         typename std::conditional<REAL, T, C2<T>>::type *tile)
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
@@ -301,26 +330,18 @@ __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
     constexpr int NI = D::NI, NO = D::NO, LL = D::LL, LPW = D::LPW, VR = D::VR;
     using TT = ColTile<T, REAL, LPW>;
     constexpr int W = TT::W, S = TT::S;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twF = reinterpret_cast<C *>(smraw);
-    C *twB = twF + D::TF;
-    E *tile = reinterpret_cast<E *>(twB + D::TB);
 
-    const int z = blockIdx.y;
-    const int c0 = blockIdx.x * W;
+    const int c0 = tx * W;
     const int nc = min(W, a.ncols - c0);
     const E *src = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane + c0;
     E *dst = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane + c0;
 
-    if (OP != OP_INV)
-        for (int i = threadIdx.x; i < D::TF; i += blockDim.x) twF[i] = a.twF[i];
-    if (OP != OP_FWD)
-        for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
     for (int idx = threadIdx.x; idx < NI * W; idx += blockDim.x) {
         const int r = idx / W, c = idx - r * W;
         E v;
-        if constexpr (REAL) v = (c < nc) ? src[(long long)r * a.src_row + c] : (T)0;
-        else v = (c < nc) ? src[(long long)r * a.src_row + c] : mk<T>(0, 0);
+        const E *p = src + (long long)r * a.src_row + c;
+        if constexpr (REAL) v = (c < nc) ? (a.ldcg ? __ldcg(p) : *p) : (T)0;
+        else v = (c < nc) ? (a.ldcg ? __ldcg(p) : *p) : mk<T>(0, 0);
         tile[sidx(r) * S + c] = v;
     }
     __syncthreads();
@@ -442,6 +463,22 @@ __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
                 d[a.ncols + 1] = tile[sidx(r) * S + 1];
             }
     }
+    __syncthreads();   // the tile may be reused by the caller's next unit
+}
+
+template <typename T, int N, int OP, bool REAL>
+__global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
+{
+    using C = C2<T>;
+    using E = typename std::conditional<REAL, T, C>::type;
+    using D = LineDerived<N, OP>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + D::TF;
+    E *tile = reinterpret_cast<E *>(twB + D::TB);
+    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
+    // (the first __syncthreads of col_unit orders these table writes before their use)
+    col_unit<T, N, OP, REAL>(a, blockIdx.y, blockIdx.x, twF, twB, tile);
 }
 
 // ----------------------------------------------------------------------------- launchers

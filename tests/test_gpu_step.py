@@ -21,9 +21,11 @@ def _alloc_step(ctx, dtype=np.float64):
 
 @pytest.mark.parametrize("prec", ["f64", "mixed"])
 @pytest.mark.parametrize("top,npz", [("neumann", 2), ("single", 1)])
-def test_step_matches_oracle(orc, prec, top, npz):
-    nx, ny, nzt = 64, 64, 65
+@pytest.mark.parametrize("fused,nx", [(1, 64), (0, 64), (1, 512)])
+def test_step_matches_oracle(orc, prec, top, npz, fused, nx):
+    ny, nzt = nx, (65 if nx == 64 else 9)
     ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
+    ctx.set_param("fused", fused)
     g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
     f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
     u, v, w = (f[k].copy(order="F") for k in "uvw")
