@@ -54,7 +54,7 @@ struct obl_ctx {
     DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
     DevBuf fscr;               // cluster scratch slots of the fused forward kernel
     // tuning parameters (obl_set_param)
-    long long param_fused = 1;          // use the cluster-fused kernels in obl_step
+    long long param_fused = 0;          // use the cluster-fused kernels in obl_step
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
     long long param_fwd_csize = 8;      // CTAs per cluster
     std::vector<DevBuf> stage; // host-variant staging (storage type)

@@ -132,11 +132,20 @@ template <typename T> struct TilePair {
     }
 };
 __host__ __device__ constexpr int tile_rows(int n) { return n + n / 8 + 1; }
+// Line-minor scratch: element i of line l at p[i*WB + l].  Threads of a warp address
+// consecutive lines of one or a few elements, so every access is bank-conflict free.
+template <typename C, int WB> struct LineMinor {
+    C *p; int l;
+    __device__ __forceinline__ C ld(int i) const { return p[i * WB + l]; }
+    __device__ __forceinline__ void st(int i, C v) { p[i * WB + l] = v; }
+};
 
 // ----------------------------------------------------------------------------- passes
 // one radix-R pass; IN_REGS: inputs already in v (D(R)), else loaded from scratch;
 // OUT_REGS: outputs stay in v (only legal for the last pass), else stored to scratch.
-template <int N, int R, int NS, int LL, bool FWD, bool IN_REGS, bool OUT_REGS, typename C, class SC>
+// BS: the lines' scratch is shared by threads of several warps (line-minor column layout),
+// so passes are separated by __syncthreads() instead of __syncwarp().
+template <int N, int R, int NS, int LL, bool FWD, bool IN_REGS, bool OUT_REGS, bool BS, typename C, class SC>
 __device__ __forceinline__ void pass(C *v, SC &sc, const C *twb, int t)
 {
     constexpr int NB = N / R;
@@ -151,7 +160,8 @@ __device__ __forceinline__ void pass(C *v, SC &sc, const C *twb, int t)
                 for (int r = 0; r < R; ++r) v[b * R + r] = sc.ld(j + r * NB);
             }
         }
-        __syncwarp();
+        if constexpr (BS) __syncthreads();
+        else __syncwarp();
     }
 #pragma unroll
     for (int b = 0; b < PER; ++b) {
@@ -173,27 +183,30 @@ __device__ __forceinline__ void pass(C *v, SC &sc, const C *twb, int t)
             }
         }
     }
-    if constexpr (!OUT_REGS) __syncwarp();
+    if constexpr (!OUT_REGS) {
+        if constexpr (BS) __syncthreads();
+        else __syncwarp();
+    }
 }
 
-template <int N, int NS, int LL, bool FWD, bool FIRST, typename C, class SC, int R0, int... Rs>
+template <int N, int NS, int LL, bool FWD, bool FIRST, bool BS, typename C, class SC, int R0, int... Rs>
 __device__ __forceinline__ void chain(C *v, SC &sc, const C *tw, int t, RPlan<R0, Rs...>)
 {
     constexpr bool LAST = sizeof...(Rs) == 0;
-    pass<N, R0, NS, LL, FWD, FIRST, LAST>(v, sc, tw, t);
+    pass<N, R0, NS, LL, FWD, FIRST, LAST, BS>(v, sc, tw, t);
     if constexpr (!LAST) {
         constexpr int adv = (NS > 1) ? R0 * NS : 0;
-        chain<N, NS * R0, LL, FWD, false, C>(v, sc, tw + adv, t, RPlan<Rs...>{});
+        chain<N, NS * R0, LL, FWD, false, BS, C>(v, sc, tw + adv, t, RPlan<Rs...>{});
     }
 }
 
 // Transform the line held in v (layout D(first radix of P)); result in D(last radix).
 // sc: scratch accessor of at least N elements; tw: the plan's twiddle table.
-template <int N, class P, int LL, bool FWD, typename C, class SC>
+template <int N, class P, int LL, bool FWD, bool BS = false, typename C, class SC>
 __device__ __forceinline__ void fft_regs(C *v, SC &sc, const C *tw, int t)
 {
     static_assert(PlanInfo<P>::product == N, "plan does not multiply to N");
-    chain<N, 1, LL, FWD, true, C>(v, sc, tw, t, P{});
+    chain<N, 1, LL, FWD, true, BS, C>(v, sc, tw, t, P{});
 }
 
 // D(R) geometry helpers

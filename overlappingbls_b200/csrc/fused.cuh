@@ -172,7 +172,7 @@ template <typename T, int N> struct FwdFusedGeo {
 };
 
 template <typename T, int N>
-__global__ void __launch_bounds__(256) k_fwd_fused(FwdFusedArgs<T> a)
+__global__ void __launch_bounds__(256, 2) k_fwd_fused(FwdFusedArgs<T> a)
 {
     using C = C2<T>;
     using GG = FwdFusedGeo<T, N>;
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_fwd_fused(FwdFusedArgs<T> a)
                 if (task < np) {
                     ColArgs<T> ca{};
                     ca.src = xpad; ca.dst = a.big[fi] + plb * z; ca.src_row = N2; ca.dst_row = N2;
-                    ca.ncols = N2; ca.nlev = 1; ca.scale = (T)1 / (T)N; ca.ldcg = 1;
+                    ca.ncols = N2; ca.nlev = 1; ca.scale = (T)1 / (T)N;
                     ca.twF = twF; ca.twB = twPB;
                     col_unit<T, N, OP_PAD, true>(ca, 0, task, twF, twPB, reinterpret_cast<T *>(work));
                 } else if (task < np + nd) {
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(256) k_fwd_fused(FwdFusedArgs<T> a)
                 } else {
                     ColArgs<T> ca{};
                     ca.src = xspec; ca.dst = a.H[fi] + sp * z; ca.src_row = LH; ca.dst_row = LH;
-                    ca.ncols = LH; ca.nlev = 1; ca.scale = (T)1; ca.zero_nyq = 1; ca.ldcg = 1;
+                    ca.ncols = LH; ca.nlev = 1; ca.scale = (T)1; ca.zero_nyq = 1;
                     col_unit<T, N, OP_FWD, false>(ca, 0, task - np - nd, twF, twB, reinterpret_cast<C *>(work));
                 }
             }

@@ -55,8 +55,6 @@ template <typename T> struct ColArgs {
     int pad_copy;                    // UNPAD: also write columns 0,1 into ncols, ncols+1
     int zero_nyq;                    // FWD: zero the Nyquist row (203_fftn_mpi.f90:33)
     int kmul;                        // INV: 0 none, 1 multiply by i*kx(col), 2 by i*ky(row)
-    int ldcg;                        // load the source with ld.global.cg (L2 only): the source
-                                     // was written by other CTAs since this SM last read it
 };
 
 // ----------------------------------------------------------------------------- configuration
@@ -336,13 +334,31 @@ __device__ __forceinline__ void col_unit(const ColArgs<T> &a, int z, int tx, con
     const E *src = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane + c0;
     E *dst = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane + c0;
 
-    for (int idx = threadIdx.x; idx < NI * W; idx += blockDim.x) {
-        const int r = idx / W, c = idx - r * W;
-        E v;
-        const E *p = src + (long long)r * a.src_row + c;
-        if constexpr (REAL) v = (c < nc) ? (a.ldcg ? __ldcg(p) : *p) : (T)0;
-        else v = (c < nc) ? (a.ldcg ? __ldcg(p) : *p) : mk<T>(0, 0);
-        tile[sidx(r) * S + c] = v;
+    // Tile load: 256 threads, UNR independent L2-only loads (ld.global.cg) in flight per
+    // thread before the shared-memory stores, so the loop is not latency-serialised.
+    // L2-only loads are also what the cluster-fused kernels need for data other CTAs wrote.
+    {
+        constexpr int TOT = NI * W, PERT = (TOT + 255) / 256, UNR = PERT < 8 ? PERT : 8;
+#pragma unroll 1
+        for (int b0 = 0; b0 < PERT; b0 += UNR) {
+            E buf[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const int idx = threadIdx.x + 256 * (b0 + u);
+                const int r = idx / W, c = idx - r * W;
+                E v;
+                if constexpr (REAL) v = (T)0;
+                else v = mk<T>(0, 0);
+                if (idx < TOT && c < nc) v = __ldcg(src + (long long)r * a.src_row + c);
+                buf[u] = v;
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const int idx = threadIdx.x + 256 * (b0 + u);
+                const int r = idx / W, c = idx - r * W;
+                if (idx < TOT) tile[sidx(r) * S + c] = buf[u];
+            }
+        }
     }
     __syncthreads();
 
@@ -481,6 +497,157 @@ __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
     col_unit<T, N, OP, REAL>(a, blockIdx.y, blockIdx.x, twF, twB, tile);
 }
 
+// ----------------------------------------------------------------------------- line-minor columns
+// Column lines without a staging tile: a CTA owns WB adjacent complex lines (WB real
+// column pairs, or WB complex columns) of one plane.  Lane l % WB is the line and the
+// remaining lane bits and the warp index form the butterfly slot t (LL slots), so
+//   * the first pass loads its operands straight from global memory: for every element
+//     index the WB lanes of a line group read WB adjacent pairs (coalesced, 8/16-byte
+//     vector loads), and the last pass stores the same way;
+//   * the exchange scratch is line-minor (element i of line l at buf[i*WB + l]): a warp
+//     always touches consecutive words, so no pass has bank conflicts;
+//   * passes are separated by __syncthreads() because a line spans all warps.
+template <typename T> struct LmGeo {
+    static constexpr int WB = sizeof(T) == 4 ? 8 : 4;   // lines per CTA (64-byte row segments)
+    static constexpr int NW = 8;                          // warps per CTA
+    static constexpr int LL = (32 / WB) * NW;             // butterfly slots per line
+};
+
+template <typename T, int N, int OP> struct ColDerived {
+    using D = LineDerived<N, OP>;
+    static constexpr int LL = LmGeo<T>::LL;
+    static constexpr int rf = Regs<D::NI, LL, typename D::PF>::v, rb = Regs<D::NO, LL, typename D::PB>::v;
+    static constexpr int VR = rf > rb ? rf : rb;
+};
+
+template <typename T, int N, int OP, bool REAL>
+__global__ void __launch_bounds__(256) k_cols2(ColArgs<T> a)
+{
+    using C = C2<T>;
+    using E = typename std::conditional<REAL, T, C>::type;
+    using D = LineDerived<N, OP>;
+    using G = LmGeo<T>;
+    constexpr int NI = D::NI, NO = D::NO, WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP>::VR;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + D::TF;
+    C *buf = twB + D::TB;
+    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int line = lane % WB, t = lane / WB + (32 / WB) * warp;
+    const int gl = blockIdx.x * WB + line;                 // global line index
+    const int nlines = REAL ? a.ncols / 2 : a.ncols;
+    const bool act = gl < nlines;
+    const int glc = act ? gl : 0;
+    const int z = blockIdx.y;
+    // element i of this line: a complex value (a real column pair for REAL)
+    const E *srcz = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane;
+    E *dstz = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane;
+    auto gld = [&](int i) -> C {
+        if constexpr (REAL) return __ldcg(reinterpret_cast<const C *>(srcz + (long long)i * a.src_row + 2 * glc));
+        else return __ldcg(srcz + (long long)i * a.src_row + glc);
+    };
+    auto gst = [&](int i, C v) {
+        if constexpr (REAL) *reinterpret_cast<C *>(dstz + (long long)i * a.dst_row + 2 * gl) = v;
+        else dstz[(long long)i * a.dst_row + gl] = v;
+    };
+    LineMinor<C, WB> sc{buf, line};
+    C v[VR];
+    C cref = mk<T>(0, 0);
+
+    if constexpr (OP != OP_INV) {
+        using GG = Geo<NI, D::RF0, LL>;
+        if constexpr (REAL) cref = gld(0);
+#pragma unroll
+        for (int b = 0; b < GG::PER; ++b) {
+            const int j = t + LL * b;
+#pragma unroll
+            for (int r = 0; r < D::RF0; ++r) {
+                C x = mk<T>(0, 0);
+                if (act && (GG::FULL || j < GG::NB)) {
+                    x = gld(j + r * GG::NB);
+                    x.x = (x.x - cref.x) * a.scale;
+                    x.y = (x.y - cref.y) * a.scale;
+                }
+                v[b * D::RF0 + r] = x;
+            }
+        }
+        fft_regs<NI, typename D::PF, LL, true, true>(v, sc, twF, t);
+    }
+    if constexpr (OP == OP_FWD) {
+        using GG = Geo<NI, D::RFL, LL>;
+        if (act) {
+#pragma unroll
+            for (int b = 0; b < GG::PER; ++b) {
+                const int j = t + LL * b;
+                if (GG::FULL || j < GG::NB)
+#pragma unroll
+                    for (int r = 0; r < D::RFL; ++r) {
+                        const int i = j + r * GG::NB;
+                        C x = v[b * D::RFL + r];
+                        if (a.zero_nyq && i == NI / 2) x = mk<T>(0, 0);
+                        gst(i, x);
+                    }
+            }
+        }
+    } else {
+        C w[VR];
+        C *vb = v;
+        if constexpr (OP == OP_INV) {
+            using GG = Geo<NO, D::RB0, LL>;
+#pragma unroll
+            for (int b = 0; b < GG::PER; ++b) {
+                const int j = t + LL * b;
+#pragma unroll
+                for (int r = 0; r < D::RB0; ++r) {
+                    const int i = j + r * GG::NB;
+                    C x = mk<T>(0, 0);
+                    if (act && (GG::FULL || j < GG::NB)) {
+                        x = gld(i);
+                        if (a.kmul) {
+                            const T kk = (T)(a.kmul == 1 ? a.ktab[glc] : a.ktab[i]);
+                            x = mk<T>(-kk * x.y, kk * x.x);
+                        }
+                        x.x *= a.scale;
+                        x.y *= a.scale;
+                    }
+                    v[b * D::RB0 + r] = x;
+                }
+            }
+        }
+        if constexpr (OP == OP_DERIV) reg_deriv<T, N, D::RFL, LL>(v, a.ktab, t);
+        if constexpr (OP == OP_PAD) { reg_pad<T, N, D::RFL, LL>(v, w, t); vb = w; }
+        if constexpr (OP == OP_UNPAD) { reg_unpad<T, N, D::RB0, LL>(v, w, t); vb = w; }
+        fft_regs<NO, typename D::PB, LL, false, true>(vb, sc, twB, t);
+        using GG = Geo<NO, D::RBL, LL>;
+        const bool addc = (OP == OP_PAD || OP == OP_UNPAD);
+        if (act) {
+#pragma unroll
+            for (int b = 0; b < GG::PER; ++b) {
+                const int j = t + LL * b;
+                if (GG::FULL || j < GG::NB)
+#pragma unroll
+                    for (int r = 0; r < D::RBL; ++r) {
+                        const int i = j + r * GG::NB;
+                        C x = vb[b * D::RBL + r];
+                        if (addc) {
+                            x.x += cref.x;
+                            x.y += cref.y;
+                        }
+                        gst(i, x);
+                        if constexpr (OP == OP_UNPAD && REAL) {
+                            // var(nxt+1:ldx,:) = var(1:2,:) (108_01_padd.f90:195)
+                            if (a.pad_copy && gl == 0)
+                                *reinterpret_cast<C *>(dstz + (long long)i * a.dst_row + a.ncols) = x;
+                        }
+                    }
+            }
+        }
+    }
+}
+
 // ----------------------------------------------------------------------------- launchers
 template <typename T, int N, int OP> inline size_t rows_smem()
 {
@@ -518,18 +685,25 @@ template <typename T, int N, int OP> cudaError_t launch_rows_t(const RowArgs<T> 
     return cudaGetLastError();
 }
 
+template <typename T, int N, int OP> inline size_t cols2_smem()
+{
+    using D = LineDerived<N, OP>;
+    return sizeof(C2<T>) * ((size_t)D::TF + D::TB + (size_t)D::NM * LmGeo<T>::WB);
+}
+
 template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const ColArgs<T> &a, cudaStream_t s)
 {
     static bool init = false;
-    const size_t sm = cols_smem<T, N, OP, REAL>();
-    auto kern = k_cols<T, N, OP, REAL>;
+    const size_t sm = cols2_smem<T, N, OP>();
+    auto kern = k_cols2<T, N, OP, REAL>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         init = true;
     }
-    constexpr int W = ColTile<T, REAL, LineDerived<N, OP>::LPW>::W;
-    dim3 grid((a.ncols + W - 1) / W, a.nlev);
+    constexpr int WB = LmGeo<T>::WB;
+    const int nlines = REAL ? a.ncols / 2 : a.ncols;
+    dim3 grid((nlines + WB - 1) / WB, a.nlev);
     if (grid.x < 1 || grid.y < 1) return cudaSuccess;
     kern<<<grid, 256, sm, s>>>(a);
     return cudaGetLastError();
