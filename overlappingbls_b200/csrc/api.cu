@@ -254,8 +254,9 @@ template <typename T> struct Ops {
     // z-difference is taken inside the solve in its own precision
     // rhs_ready: H_x, H_y, H_z at levels 1..L were already produced (by the fused
     // forward kernel); only the boundary planes H_z(0), H_z(nz) are transformed here.
+    // proj: when given (with dpdz_out), the inverse is fused with project() on proj->u,v,w
     int press(const T *u, const T *v, const T *w, const T *dbot, const T *dtop, T *p, T *dpdx, T *dpdy,
-              T *dpdz_out = nullptr, bool rhs_ready = false)
+              T *dpdz_out = nullptr, bool rhs_ready = false, const obl_step_io *proj = nullptr)
     {
         const long long S = ctx->sp();
         const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
@@ -329,6 +330,36 @@ template <typename T> struct Ops {
                 launch_tdma_island<T>(ta, isl, s(), e);
                 if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_island");
             }
+        }
+        if (proj && dpdz_out) {
+            // fused inverse + project: one y-inverse pass over p_hat and the dpdz spectrum,
+            // one x-inverse pass over the rows that also applies project()
+            PinvColArgs<T> pc{};
+            pc.ph = ph; pc.dph = (const C2<T> *)ctx->spec[4].p;
+            pc.Xp = Hz; pc.Xdx = Hx; pc.Xdy = Hy; pc.Xdz = (C2<T> *)ctx->spec[4].p;
+            pc.S = S; pc.lhx = lhx; pc.kx = ctx->d_kx; pc.ky = ctx->d_ky2;
+            pc.twB = twt<T>(ctx, ny, ROLE_BWD);
+            {
+                LaunchScope ls(ctx->rec, "pinv_cols", s());
+                if ((rc = chk(PinvLaunch<T>::cols(ny, pc, L + 1, s()), "pinv_cols"))) return rc;
+            }
+            PinvRowArgs<T> pr{};
+            pr.Xp = Hz; pr.Xdx = Hx; pr.Xdy = Hy; pr.Xdz = (const C2<T> *)ctx->spec[4].p;
+            pr.p = p; pr.dpdx = dpdx; pr.dpdy = dpdy; pr.dpdz = dpdz_out;
+            pr.u = (T *)proj->u; pr.v = (T *)proj->v; pr.w = (T *)proj->w;
+            pr.npairs = (long long)ny * (L + 1) / 2;
+            pr.ldx = ldx; pr.ny = ny; pr.lhx = lhx;
+            pr.dt_tadv1 = (T)(ctx->dt_nd * kTadv1);
+            pr.twB = twt<T>(ctx, nx, ROLE_BWD);
+            {
+                LaunchScope ls(ctx->rec, "pinv_rows_project", s());
+                if ((rc = chk(PinvLaunch<T>::rows(nx, pr, s()), "pinv_rows_project"))) return rc;
+            }
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "project_bc", s());
+            launch_project_bc<T>((T *)proj->u, (T *)proj->v, (T *)proj->w, ldx, ny, ctx->nz,
+                                 (int)ctx->opt.ubc_stress_free, s(), e);
+            return chk(e, "project_bc");
         }
         // inverse transforms (:231-238): p at 0..L, dpdx/dpdy at 1..L; Hx/Hy/Hz are
         // free now and hold the y-inverses
@@ -416,18 +447,56 @@ template <typename T> struct Ops {
         return chk(FwdFusedLaunch<T>::run(n, a, ncl, csize, s()), "fwd_fused");
     }
 
+    // line-kernel forward pass of the step: per field one multi-output row pass (ddx,
+    // x-pad, RHS x-spectrum) and the column passes (y-pad, ddy, RHS y-transform)
+    int fwd_lines(const obl_step_io *io)
+    {
+        const int nlev = ctx->nz + 1, nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        const long long S = ctx->sp();
+        const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
+        int rc;
+        for (int i = 0; i < 5; ++i)
+            if ((rc = ensure(ctx, ctx->spec[i], sb))) return rc;
+        if ((rc = ensure(ctx, ctx->tmp, sizeof(T) * (size_t)nx2 * ny * nlev))) return rc;
+        T *xb = (T *)ctx->tmp.p;
+        const T *f[4] = {(const T *)io->u, (const T *)io->v, (const T *)io->w, (const T *)io->theta};
+        const double scp = ((1.0 / ((double)nx * ny)) / kTadv1) * (1.0 / ctx->dt_nd);
+        for (int c = 0; c < 4; ++c) {
+            C2<T> *H = c < 3 ? (C2<T> *)ctx->spec[c].p : nullptr;
+            RowsFwd3Args<T> ra{};
+            ra.src = f[c]; ra.dfdx = (T *)io->d[2 * c]; ra.xpad = xb; ra.H = H;
+            ra.npairs = (long long)ny * nlev / 2; ra.ldx = ctx->ldx; ra.ny = ny; ra.L = ctx->L;
+            ra.sc_press = scp; ra.kx = ctx->d_kx;
+            ra.twF = twt<T>(ctx, nx, ROLE_FWD); ra.twB = twt<T>(ctx, nx, ROLE_BWD);
+            ra.twPB = twt<T>(ctx, nx, ROLE_PADBWD);
+            {
+                LaunchScope ls(ctx->rec, "rows_fwd3", s());
+                if ((rc = chk(RowsFwd3Launch<T>::run(nx, ra, s()), "rows_fwd3"))) return rc;
+            }
+            auto ca = colargs(xb, nx2, (long long)nx2 * ny, io->big[c], nx2, (long long)nx2 * ny2, nx2, nlev,
+                              1.0 / ny, OP_PAD, ny);
+            if ((rc = cols(OP_PAD, true, ny, ca, "pad_cols"))) return rc;
+            if ((rc = ddy((T *)io->d[2 * c + 1], f[c], nlev))) return rc;
+            if (H) {
+                auto cb = colargs(H + S, ctx->lhx, S, H + S, ctx->lhx, S, ctx->lhx, ctx->L, 1.0, OP_FWD, ny);
+                cb.zero_nyq = 1;
+                if ((rc = cols(OP_FWD, false, ny, cb, "press_fwd_cols"))) return rc;
+            }
+        }
+        return OBL_OK;
+    }
+
     int step(const obl_step_io *io)
     {
         const int nlev = ctx->nz + 1;
         const T *f[4] = {(const T *)io->u, (const T *)io->v, (const T *)io->w, (const T *)io->theta};
         int rc;
-        if (ctx->param_fused && ctx->nxt == ctx->nyt) {
-            if ((rc = fwd_fused(io))) return rc;
-            if ((rc = press(f[0], f[1], f[2], (const T *)io->divtz_bot, (const T *)io->divtz_top, (T *)io->p,
-                            (T *)io->dp[0], (T *)io->dp[1], (T *)io->dp[2], true)))
-                return rc;
-            return project((T *)io->u, (T *)io->v, (T *)io->w, (const T *)io->dp[0], (const T *)io->dp[1],
-                           (const T *)io->dp[2]);
+        // param "fused": 0 multi-output line kernels (default), 1 cluster-fused forward pass,
+        // 2 the plain composition of the per-routine entry points
+        if (ctx->param_fused == 0 || (ctx->param_fused == 1 && ctx->nxt == ctx->nyt)) {
+            if ((rc = ctx->param_fused == 0 ? fwd_lines(io) : fwd_fused(io))) return rc;
+            return press(f[0], f[1], f[2], (const T *)io->divtz_bot, (const T *)io->divtz_top, (T *)io->p,
+                         (T *)io->dp[0], (T *)io->dp[1], (T *)io->dp[2], true, io);
         }
         for (int c = 0; c < 4; ++c) {
             if ((rc = ddx((T *)io->d[2 * c], f[c], nlev))) return rc;

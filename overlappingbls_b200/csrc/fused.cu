@@ -101,4 +101,100 @@ template <typename T> int FwdFusedLaunch<T>::max_clusters(int n, int csize)
 template struct FwdFusedLaunch<float>;
 template struct FwdFusedLaunch<double>;
 
+template <typename T, int N> static cudaError_t rows3_run_n(const RowsFwd3Args<T> &a, cudaStream_t s)
+{
+    using GG = FwdFusedGeo<T, N>;
+    const size_t sm = sizeof(C2<T>) * ((size_t)GG::TF + GG::TB + GG::TPB) + GG::row_scr;
+    static int cap = 0;
+    auto kern = k_rows_fwd3<T, N>;
+    if (!cap) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        int dev = 0, nsm = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
+        cap = nsm * (per > 0 ? per : 1);
+    }
+    const long long per_cta = 8LL * GG::LPW;
+    const long long want = (a.npairs + per_cta - 1) / per_cta;
+    const int grid = (int)(want < cap ? want : cap);
+    if (grid < 1) return cudaSuccess;
+    kern<<<grid, 256, sm, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T> cudaError_t RowsFwd3Launch<T>::run(int n, const RowsFwd3Args<T> &a, cudaStream_t s)
+{
+    switch (n) {
+#define OBL_CASE(N) case N: return rows3_run_n<T, N>(a, s);
+        OBL_FOR_EACH_N(OBL_CASE)
+#undef OBL_CASE
+    }
+    return cudaErrorNotSupported;
+}
+
+template struct RowsFwd3Launch<float>;
+template struct RowsFwd3Launch<double>;
+
+template <typename T, int N> static cudaError_t pinv_cols_n(const PinvColArgs<T> &a, int nlev, cudaStream_t s)
+{
+    using D = LineDerived<N, OP_INV>;
+    const size_t sm = sizeof(C2<T>) * ((size_t)D::TB + (size_t)N * LmGeo<T>::WB);
+    static bool init = false;
+    auto kern = k_cols_pinv<T, N>;
+    if (!init) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        init = true;
+    }
+    dim3 grid((a.lhx + LmGeo<T>::WB - 1) / LmGeo<T>::WB, nlev);
+    kern<<<grid, 256, sm, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T, int N> static cudaError_t pinv_rows_n(const PinvRowArgs<T> &a, cudaStream_t s)
+{
+    using D = LineDerived<N, OP_INV>;
+    const size_t sm = sizeof(C2<T>) * ((size_t)D::TB + (size_t)8 * D::LPW * scratch_len(N));
+    static int cap = 0;
+    auto kern = k_rows_pinv<T, N>;
+    if (!cap) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        int dev = 0, nsm = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
+        cap = nsm * (per > 0 ? per : 1);
+    }
+    const long long per_cta = 8LL * D::LPW;
+    const long long want = (a.npairs + per_cta - 1) / per_cta;
+    const int grid = (int)(want < cap ? want : cap);
+    if (grid < 1) return cudaSuccess;
+    kern<<<grid, 256, sm, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T> cudaError_t PinvLaunch<T>::cols(int n, const PinvColArgs<T> &a, int nlev, cudaStream_t s)
+{
+    switch (n) {
+#define OBL_CASE(N) case N: return pinv_cols_n<T, N>(a, nlev, s);
+        OBL_FOR_EACH_N(OBL_CASE)
+#undef OBL_CASE
+    }
+    return cudaErrorNotSupported;
+}
+template <typename T> cudaError_t PinvLaunch<T>::rows(int n, const PinvRowArgs<T> &a, cudaStream_t s)
+{
+    switch (n) {
+#define OBL_CASE(N) case N: return pinv_rows_n<T, N>(a, s);
+        OBL_FOR_EACH_N(OBL_CASE)
+#undef OBL_CASE
+    }
+    return cudaErrorNotSupported;
+}
+template struct PinvLaunch<float>;
+template struct PinvLaunch<double>;
+
 } // namespace obl

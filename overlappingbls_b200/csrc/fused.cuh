@@ -251,6 +251,265 @@ __global__ void __launch_bounds__(256, 2) k_fwd_fused(FwdFusedArgs<T> a)
     }
 }
 
+// ----------------------------------------------------------------------------- multi-output rows
+// One read of each row pair of a field yields ddx, the x-padded rows (zero_padding's
+// first half, into the intermediate xpad) and, on levels 1..L of u, v, w, the scaled x
+// half-spectra of the pressure RHS (written straight into H; the y transform then runs
+// in place).  Replaces three separate row passes over the same field.
+template <typename T> struct RowsFwd3Args {
+    const T *src;          // field (ldx, ny, nlev)
+    T *dfdx;               // (ldx, ny, nlev)
+    T *xpad;               // (nx2, ny, nlev)
+    C2<T> *H;              // (lhx, ny, nlev) or nullptr (theta)
+    long long npairs;      // ny*nlev/2
+    int ldx, ny, L;
+    double sc_press;
+    const double *kx;
+    const C2<T> *twF, *twB, *twPB;
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_rows_fwd3(RowsFwd3Args<T> a)
+{
+    using C = C2<T>;
+    using GG = FwdFusedGeo<T, N>;
+    constexpr int N2 = GG::N2, LH = GG::LH, LPW = GG::LPW;
+    constexpr int LL = GG::DD::LL;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + GG::TF;
+    C *twPB = twB + GG::TB;
+    C *scr = twPB + GG::TPB;
+    for (int i = threadIdx.x; i < GG::TF; i += blockDim.x) twF[i] = a.twF[i];
+    for (int i = threadIdx.x; i < GG::TB; i += blockDim.x) twB[i] = a.twB[i];
+    for (int i = threadIdx.x; i < GG::TPB; i += blockDim.x) twPB[i] = a.twPB[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int g = lane / LL, t = lane % LL;
+    C *line = scr + (warp * LPW + g) * scratch_len(N2);
+    for (long long base = ((long long)blockIdx.x * nw + warp) * LPW; base < a.npairs;
+         base += (long long)gridDim.x * nw * LPW) {
+        const long long p = base + g;
+        const bool act = p < a.npairs;
+        const long long r0 = 2 * (act ? p : base);
+        // warp-uniform: the LPW pairs of a warp lie on one level (ny/2 is a multiple of LPW)
+        const int zw = (int)((2 * base) / a.ny);
+        const bool spec = a.H != nullptr && zw >= 1 && zw <= a.L;
+        const T *A = a.src + r0 * a.ldx;
+        T *dA = a.dfdx + r0 * a.ldx;
+        T *pA = a.xpad + r0 * N2;
+        C *sA = spec ? a.H + r0 * LH : nullptr;
+        C *sB = spec ? a.H + (r0 + 1) * LH : nullptr;
+        row_fwd_fused<T, N>(A, A + a.ldx, dA, dA + a.ldx, pA, pA + N2, sA, sB, act, spec, a.sc_press, a.kx,
+                            twF, twB, twPB, line, t);
+    }
+}
+
+template <typename T> struct RowsFwd3Launch {
+    static cudaError_t run(int n, const RowsFwd3Args<T> &a, cudaStream_t s);
+};
+
+// ----------------------------------------------------------------------------- fused inverse
+// y-inverse of the pressure solution: one load of p_hat(z) gives the y-inverses of p_hat,
+// i*kx*p_hat and i*ky*p_hat (109_press_stag_array.f90:231-238), one load of the dpdz
+// spectrum gives its y-inverse.  Level 0 only needs p.  Line-minor column layout.
+template <typename T> struct PinvColArgs {
+    const C2<T> *ph, *dph;                // (lhx, ny, 0..L) spectra
+    C2<T> *Xp, *Xdx, *Xdy, *Xdz;          // y-inverses, same layout
+    long long S;                          // lhx*ny
+    int lhx;
+    const double *kx, *ky;                // kx(lhx), ky_2d row (ny)
+    const C2<T> *twB;
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_cols_pinv(PinvColArgs<T> a)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP_INV>;
+    using G = LmGeo<T>;
+    constexpr int WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP_INV>::VR;
+    constexpr int R0 = D::RB0, RL = D::RBL;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twB = reinterpret_cast<C *>(smraw);
+    C *buf = twB + D::TB;
+    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int line = lane % WB, t = lane / WB + (32 / WB) * warp;
+    const int gl = blockIdx.x * WB + line;
+    const bool act = gl < a.lhx;
+    const int glc = act ? gl : 0;
+    const int z = blockIdx.y;
+    LineMinor<C, WB> sc{buf, line};
+    using G0 = Geo<N, R0, LL>;
+    using GL = Geo<N, RL, LL>;
+    auto load = [&](const C *src, C *v) {
+#pragma unroll
+        for (int b = 0; b < G0::PER; ++b) {
+            const int j = t + LL * b;
+#pragma unroll
+            for (int r = 0; r < R0; ++r) {
+                const int i = j + r * G0::NB;
+                v[b * R0 + r] = (act && (G0::FULL || j < G0::NB)) ? __ldcg(src + a.S * z + (long long)i * a.lhx + glc)
+                                                                   : mk<T>(0, 0);
+            }
+        }
+    };
+    auto store = [&](C *dst, const C *v) {
+        if (!act) return;
+#pragma unroll
+        for (int b = 0; b < GL::PER; ++b) {
+            const int j = t + LL * b;
+            if (GL::FULL || j < GL::NB)
+#pragma unroll
+                for (int r = 0; r < RL; ++r) dst[a.S * z + (long long)(j + r * GL::NB) * a.lhx + gl] = v[b * RL + r];
+        }
+    };
+    C v[VR], w[VR];
+    load(a.ph, v);
+    // i*ky(row) and i*kx(col) multipliers act element-wise on the loaded layout
+#pragma unroll
+    for (int q = 0; q < VR; ++q) w[q] = v[q];
+    fft_regs<N, typename D::PB, LL, false, true>(w, sc, twB, t);
+    store(a.Xp, w);
+    if (z == 0) return;   // uniform per block
+    const T kxv = (T)a.kx[glc];
+#pragma unroll
+    for (int q = 0; q < VR; ++q) w[q] = mk<T>(-kxv * v[q].y, kxv * v[q].x);
+    fft_regs<N, typename D::PB, LL, false, true>(w, sc, twB, t);
+    store(a.Xdx, w);
+#pragma unroll
+    for (int b = 0; b < G0::PER; ++b) {
+        const int j = t + LL * b;
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+            const int i = (G0::FULL || j < G0::NB) ? j + r * G0::NB : 0;
+            const T kyv = (T)a.ky[i];
+            const C x = v[b * R0 + r];
+            w[b * R0 + r] = mk<T>(-kyv * x.y, kyv * x.x);
+        }
+    }
+    fft_regs<N, typename D::PB, LL, false, true>(w, sc, twB, t);
+    store(a.Xdy, w);
+    load(a.dph, w);
+    fft_regs<N, typename D::PB, LL, false, true>(w, sc, twB, t);
+    store(a.Xdz, w);
+}
+
+// x-inverse of the four y-inverses and the projection (110_project.f90:16-40) in one
+// pass over the rows: p at levels 0..L, dpdx/dpdy/dpdz at 1..L (slot z-1), and
+// u,v (levels 1..L) and w (levels 2..L) += dt*(-tadv1*grad p).
+template <typename T> struct PinvRowArgs {
+    const C2<T> *Xp, *Xdx, *Xdy, *Xdz;    // (lhx, ny, 0..L)
+    T *p, *dpdx, *dpdy, *dpdz;            // p (ldx, ny, 0:nz); d* (ldx, ny, 1:nz)
+    T *u, *v, *w;                         // updated in place (ldx, ny, 0:nz)
+    long long npairs;                     // ny*(L+1)/2
+    int ldx, ny, lhx;
+    T dt_tadv1;                           // dt*tadv1
+    const C2<T> *twB;
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP_INV>;
+    constexpr int LL = D::LL, LPW = D::LPW, VR = D::VR, R0 = D::RB0, RL = D::RBL;
+    constexpr int SL = scratch_len(N);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twB = reinterpret_cast<C *>(smraw);
+    C *scr = twB + D::TB;
+    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int g = lane / LL, t = lane % LL;
+    LineScratch<C> sc{scr + (warp * LPW + g) * SL};
+    using G0 = Geo<N, R0, LL>;
+    using GL = Geo<N, RL, LL>;
+    const long long pl = (long long)a.ldx * a.ny;
+    for (long long base = ((long long)blockIdx.x * nw + warp) * LPW; base < a.npairs;
+         base += (long long)gridDim.x * nw * LPW) {
+        const long long pr = base + g;
+        const bool act = pr < a.npairs;
+        const long long r0 = 2 * (act ? pr : base);
+        const int zw = (int)((2 * base) / a.ny);          // warp-uniform level
+        const long long off = (r0 % a.ny) * a.ldx;        // row offset inside the level
+        const int z = (int)(r0 / a.ny);
+        // inverse of the two half-spectrum rows r0, r0+1 of X into real rows (v in D(RL))
+        auto inv = [&](const C *X, C *v) {
+            const C *A = X + r0 * a.lhx;
+            const C *B = A + a.lhx;
+#pragma unroll
+            for (int b = 0; b < G0::PER; ++b) {
+                const int j = t + LL * b;
+#pragma unroll
+                for (int r = 0; r < R0; ++r) {
+                    const int i = j + r * G0::NB;
+                    C zz = mk<T>(0, 0);
+                    if (act && (G0::FULL || j < G0::NB)) {
+                        const bool lo = i <= N / 2;
+                        const int k = lo ? i : N - i;
+                        C av = __ldcg(A + k), bv = __ldcg(B + k);
+                        if (k == 0 || k == N / 2) { av.y = 0; bv.y = 0; }
+                        zz = lo ? mk<T>(av.x - bv.y, av.y + bv.x) : mk<T>(av.x + bv.y, bv.x - av.y);
+                    }
+                    v[b * R0 + r] = zz;
+                }
+            }
+            fft_regs<N, typename D::PB, LL, false>(v, sc, twB, t);
+        };
+        auto put = [&](T *dst, const C *v) {
+            if (!act) return;
+#pragma unroll
+            for (int b = 0; b < GL::PER; ++b) {
+                const int j = t + LL * b;
+                if (GL::FULL || j < GL::NB)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int i = j + r * GL::NB;
+                        dst[i] = v[b * RL + r].x;
+                        dst[a.ldx + i] = v[b * RL + r].y;
+                    }
+            }
+        };
+        // u(z) = u(z) + dt*(-tadv1*g) for the two rows
+        auto proj = [&](T *f, const C *gv) {
+            if (!act) return;
+#pragma unroll
+            for (int b = 0; b < GL::PER; ++b) {
+                const int j = t + LL * b;
+                if (GL::FULL || j < GL::NB)
+#pragma unroll
+                    for (int r = 0; r < RL; ++r) {
+                        const int i = j + r * GL::NB;
+                        f[i] = f[i] + (-a.dt_tadv1 * gv[b * RL + r].x);
+                        f[a.ldx + i] = f[a.ldx + i] + (-a.dt_tadv1 * gv[b * RL + r].y);
+                    }
+            }
+        };
+        C v[VR];
+        inv(a.Xp, v);
+        put(a.p + pl * z + off, v);
+        if (zw == 0) continue;   // level 0: p only
+        const long long dof = pl * (z - 1) + off;
+        inv(a.Xdx, v);
+        put(a.dpdx + dof, v);
+        proj(a.u + pl * z + off, v);
+        inv(a.Xdy, v);
+        put(a.dpdy + dof, v);
+        proj(a.v + pl * z + off, v);
+        inv(a.Xdz, v);
+        put(a.dpdz + dof, v);
+        if (zw >= 2) proj(a.w + pl * z + off, v);
+    }
+}
+
+template <typename T> struct PinvLaunch {
+    static cudaError_t cols(int n, const PinvColArgs<T> &a, int nlev, cudaStream_t s);
+    static cudaError_t rows(int n, const PinvRowArgs<T> &a, cudaStream_t s);
+};
+
 template <typename T> struct FwdFusedLaunch {
     // returns cudaErrorNotSupported for lengths without an instantiation
     static cudaError_t run(int n, const FwdFusedArgs<T> &a, int nclusters, int csize, cudaStream_t s);

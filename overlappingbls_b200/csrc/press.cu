@@ -254,6 +254,14 @@ void launch_project(T *u, T *v, T *w, const T *dpdx, const T *dpdy, const T *dpd
     e = cudaGetLastError();
 }
 
+template <typename T>
+void launch_project_bc(T *u, T *v, T *w, int ldx, int nyt, int nz, int stress_free, cudaStream_t s, cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    k_project_bc<T><<<fgrid(ldx, nyt, 1), 128, 0, s>>>(u, v, w, ldx, nyt, nz, stress_free);
+    e = cudaGetLastError();
+}
+
 __global__ void k_d2f(float *d, const double *s, long long n)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -292,6 +300,7 @@ void launch_convert_f2d(double *dst, const float *src, long long n, cudaStream_t
                                   cudaError_t &);                                                    \
     template void launch_dpdz<T>(T *, const T *, int, int, int, int, double, cudaStream_t,          \
                                  cudaError_t &);                                                     \
+    template void launch_project_bc<T>(T *, T *, T *, int, int, int, int, cudaStream_t, cudaError_t &); \
     template void launch_project<T>(T *, T *, T *, const T *, const T *, const T *, int, int, int,  \
                                     int, double, int, cudaStream_t, cudaError_t &);
 OBL_INST(float)

@@ -39,6 +39,9 @@ template <typename T> void launch_ddz_w(T *dfdz, const T *fun, int nxt, int ldx,
                                         double dz, cudaStream_t s, cudaError_t &e);
 template <typename T> void launch_dpdz(T *dpdz, const T *p, int nxt, int ldx, int nyt, int nz,
                                        double dz, cudaStream_t s, cudaError_t &e);
+// only the boundary part of project (110_project.f90:50-60), after an interior update
+template <typename T> void launch_project_bc(T *u, T *v, T *w, int ldx, int nyt, int nz, int stress_free,
+                                             cudaStream_t s, cudaError_t &e);
 template <typename T> void launch_project(T *u, T *v, T *w, const T *dpdx, const T *dpdy,
                                           const T *dpdz, int nxt, int ldx, int nyt, int nz,
                                           double dt, int stress_free, cudaStream_t s,

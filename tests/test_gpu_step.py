@@ -21,7 +21,7 @@ def _alloc_step(ctx, dtype=np.float64):
 
 @pytest.mark.parametrize("prec", ["f64", "mixed"])
 @pytest.mark.parametrize("top,npz", [("neumann", 2), ("single", 1)])
-@pytest.mark.parametrize("fused,nx", [(1, 64), (0, 64), (1, 512)])
+@pytest.mark.parametrize("fused,nx", [(0, 64), (1, 64), (2, 64), (0, 512), (1, 512), (0, 96)])
 def test_step_matches_oracle(orc, prec, top, npz, fused, nx):
     ny, nzt = nx, (65 if nx == 64 else 9)
     ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
