@@ -136,7 +136,8 @@ def run_ours(args, rank, local, world):
     stream = torch.cuda.current_stream(dev)
 
     def make_ctx(prec):
-        c = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", device=local, **fields.DOMAIN)
+        c = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", device=local,
+                        fp64_k2_max=args.fp64_k2_max, **fields.DOMAIN)
         c.set_stream(stream.cuda_stream)
         for kv in args.param:
             k, v = kv.split("=")
@@ -323,6 +324,7 @@ def run_ours(args, rank, local, world):
         "config": {"workload": f"{args.workload} ({nx}x{ny}x{L} levels), {args.prec}",
                    "nxt": nx, "nyt": ny, "nzt": nzt, "points_per_instance": pts, "instances": world,
                    "precision": args.prec, "top_bc": "neumann",
+                   "fp64_columns": ctx.info["n_fp64_columns"],
                    "l2": "inputs larger than L2 (one field = %.0f MB)" % (ctx.info["field_elems"] * es / 1e6),
                    "parallelism": f"replicas x{world}"},
         "step_roofline": {"bound": "hbm", "bytes_per_step": step_bytes, "achieved": round(step_gbs, 1),
@@ -394,6 +396,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--fp64-k2-max", type=float, default=-1.0,
+                    help="mixed mode: k^2 bound of the FP64 TDMA columns (-1 = library default)")
     ap.add_argument("--param", action="append", default=[],
                     help="execution tuning name=value passed to obl_set_param (e.g. fused=0)")
     args = ap.parse_args()

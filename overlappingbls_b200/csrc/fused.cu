@@ -168,8 +168,8 @@ template <typename T, int N> static cudaError_t pinv_rows_n(const PinvRowArgs<T>
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
         cap = nsm * (per > 0 ? per : 1);
     }
-    const long long per_cta = 8LL * D::LPW;
-    const long long want = (a.npairs + per_cta - 1) / per_cta;
+    const long long items = 4 * ((a.npairs + D::LPW - 1) / D::LPW);   // (pair group, component)
+    const long long want = (items + 7) / 8;
     const int grid = (int)(want < cap ? want : cap);
     if (grid < 1) return cudaSuccess;
     kern<<<grid, 256, sm, s>>>(a);

@@ -428,16 +428,39 @@ __global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
     using G0 = Geo<N, R0, LL>;
     using GL = Geo<N, RL, LL>;
     const long long pl = (long long)a.ldx * a.ny;
-    for (long long base = ((long long)blockIdx.x * nw + warp) * LPW; base < a.npairs;
-         base += (long long)gridDim.x * nw * LPW) {
+    const long long ngroups = (a.npairs + LPW - 1) / LPW;
+    // work item wi: component q = wi % 4 (0: p; 1: dpdx and u; 2: dpdy and v; 3: dpdz and w)
+    // of the LPW row pairs of group wi / 4.  Independent items keep many row transforms in
+    // flight per SM instead of four dependent ones per warp.
+    for (long long wi = (long long)blockIdx.x * nw + warp; wi < 4 * ngroups; wi += (long long)gridDim.x * nw) {
+        const int q = (int)(wi % 4);
+        const long long base = (wi / 4) * LPW;
         const long long pr = base + g;
         const bool act = pr < a.npairs;
         const long long r0 = 2 * (act ? pr : base);
-        const int zw = (int)((2 * base) / a.ny);          // warp-uniform level
-        const long long off = (r0 % a.ny) * a.ldx;        // row offset inside the level
-        const int z = (int)(r0 / a.ny);
-        // inverse of the two half-spectrum rows r0, r0+1 of X into real rows (v in D(RL))
-        auto inv = [&](const C *X, C *v) {
+        const int z = (int)((2 * base) / a.ny);            // warp-uniform level
+        if (q > 0 && z == 0) continue;                     // level 0 holds p only
+        const long long off = (r0 % a.ny) * a.ldx;
+        const C *X = q == 0 ? a.Xp : q == 1 ? a.Xdx : q == 2 ? a.Xdy : a.Xdz;
+        T *out = q == 0 ? a.p + pl * z + off : (q == 1 ? a.dpdx : q == 2 ? a.dpdy : a.dpdz) + pl * (z - 1) + off;
+        T *f = (q == 1 ? a.u : q == 2 ? a.v : a.w) + pl * z + off;
+        const bool proj = q == 1 || q == 2 || (q == 3 && z >= 2);   // jz_min = 2 for w
+        // the two rows of the field to update are read before the transform
+        T fa[GL::PER * RL], fb[GL::PER * RL];
+#pragma unroll
+        for (int b = 0; b < GL::PER; ++b) {
+            const int j = t + LL * b;
+#pragma unroll
+            for (int r = 0; r < RL; ++r) {
+                const int i = j + r * GL::NB;
+                const bool ok = proj && act && (GL::FULL || j < GL::NB);
+                fa[b * RL + r] = ok ? f[i] : (T)0;
+                fb[b * RL + r] = ok ? f[a.ldx + i] : (T)0;
+            }
+        }
+        // two Hermitian half spectra (rows r0, r0+1 of X) -> Z = A + iB, Im of DC/Nyquist ignored
+        C v[VR];
+        {
             const C *A = X + r0 * a.lhx;
             const C *B = A + a.lhx;
 #pragma unroll
@@ -457,10 +480,9 @@ __global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
                     v[b * R0 + r] = zz;
                 }
             }
-            fft_regs<N, typename D::PB, LL, false>(v, sc, twB, t);
-        };
-        auto put = [&](T *dst, const C *v) {
-            if (!act) return;
+        }
+        fft_regs<N, typename D::PB, LL, false>(v, sc, twB, t);
+        if (act) {
 #pragma unroll
             for (int b = 0; b < GL::PER; ++b) {
                 const int j = t + LL * b;
@@ -468,43 +490,18 @@ __global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
 #pragma unroll
                     for (int r = 0; r < RL; ++r) {
                         const int i = j + r * GL::NB;
-                        dst[i] = v[b * RL + r].x;
-                        dst[a.ldx + i] = v[b * RL + r].y;
+                        const C x = v[b * RL + r];
+                        out[i] = x.x;
+                        out[a.ldx + i] = x.y;
+                        if (proj) {   // 110_project.f90:16-40: u = u + dt*(-tadv1*dpdx)
+                            f[i] = fa[b * RL + r] + (-a.dt_tadv1 * x.x);
+                            f[a.ldx + i] = fb[b * RL + r] + (-a.dt_tadv1 * x.y);
+                        }
                     }
             }
-        };
-        // u(z) = u(z) + dt*(-tadv1*g) for the two rows
-        auto proj = [&](T *f, const C *gv) {
-            if (!act) return;
-#pragma unroll
-            for (int b = 0; b < GL::PER; ++b) {
-                const int j = t + LL * b;
-                if (GL::FULL || j < GL::NB)
-#pragma unroll
-                    for (int r = 0; r < RL; ++r) {
-                        const int i = j + r * GL::NB;
-                        f[i] = f[i] + (-a.dt_tadv1 * gv[b * RL + r].x);
-                        f[a.ldx + i] = f[a.ldx + i] + (-a.dt_tadv1 * gv[b * RL + r].y);
-                    }
-            }
-        };
-        C v[VR];
-        inv(a.Xp, v);
-        put(a.p + pl * z + off, v);
-        if (zw == 0) continue;   // level 0: p only
-        const long long dof = pl * (z - 1) + off;
-        inv(a.Xdx, v);
-        put(a.dpdx + dof, v);
-        proj(a.u + pl * z + off, v);
-        inv(a.Xdy, v);
-        put(a.dpdy + dof, v);
-        proj(a.v + pl * z + off, v);
-        inv(a.Xdz, v);
-        put(a.dpdz + dof, v);
-        if (zw >= 2) proj(a.w + pl * z + off, v);
+        }
     }
 }
-
 template <typename T> struct PinvLaunch {
     static cudaError_t cols(int n, const PinvColArgs<T> &a, int nlev, cudaStream_t s);
     static cudaError_t rows(int n, const PinvRowArgs<T> &a, cudaStream_t s);

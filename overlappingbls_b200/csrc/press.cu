@@ -17,12 +17,12 @@ namespace obl {
 static constexpr double kTadv1 = 1.5;                 // 001_param.f90:152
 static constexpr double kBogus = -1234567890.0;       // 001_param.f90:40
 
+// One column's solve; t = the thread's index among the bulk columns or in the island list.
 template <typename TS, typename TC, bool ISLAND>
-__global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
+__device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandArgs &isl, long long t)
 {
     using CS = C2<TS>;
     using CC = C2<TC>;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long q;
     if constexpr (ISLAND) {
         if (t >= isl.n) return;
@@ -72,12 +72,17 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
     };
 
     // ---- forward elimination ----
+    // The RHS inputs of level iz+1 are loaded while level iz is eliminated (the loads are
+    // independent of the recurrence; issuing them ahead hides their latency).
     const CC hz0 = ld(a.Hz, 0);     // RHS_col(0) = H_z(0) (:209)
     CC hzc = ld(a.Hz, 1);
+    CC hzn = ld(a.Hz, 2);
+    CC hx = ld(a.Hx, 1), hy = ld(a.Hy, 1);
     CC dprev = hz0;
     TC cprev = 0;                   // coef_cp(0) = 0 on the bottom rank
     for (int iz = 1; iz <= L; ++iz) {
-        const CC hzn = ld(a.Hz, iz + 1);
+        const int izn = iz < L ? iz + 1 : iz;
+        const CC hx_n = ld(a.Hx, izn), hy_n = ld(a.Hy, izn), hz_n = ld(a.Hz, izn + 1);
         TC am, bm, cm;
         CC r;
         if (!m00) {
@@ -85,7 +90,6 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
             am = (iz == 1) ? (TC)0 : idz2;
             bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (TC)2 * idz2);
             cm = top ? (TC)0 : idz2;
-            const CC hx = ld(a.Hx, iz), hy = ld(a.Hy, iz);
             const CC sxy = mk<TC>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
             CC dh = csub(hzn, hzc);
             if (iz == 1) dh = cadd(dh, hz0);
@@ -97,23 +101,34 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
             r = (iz == 1) ? mk<TC>(0, 0) : hzc;
         }
         const TC bp = bm - am * cprev;
-        const TC cp = cm / bp;
-        const CC d = mk<TC>((r.x - am * dprev.x) / bp, (r.y - am * dprev.y) / bp);
+        const TC ibp = (TC)1 / bp;
+        const TC cp = cm * ibp;
+        const CC d = mk<TC>((r.x - am * dprev.x) * ibp, (r.y - am * dprev.y) * ibp);
         st_c(iz, cp);
         st_d(iz, d);
         cprev = cp;
         dprev = d;
         hzc = hzn;
+        hzn = hz_n;
+        hx = hx_n;
+        hy = hy_n;
     }
     // ---- back substitution ----
     CC pn = a.neumann_top ? dprev : mk<TC>(0, 0);   // p_hat(nz-1): solved row / forced 0
     ph[S * L] = mk<TS>((TS)pn.x, (TS)pn.y);
     C2<TS> *dph = a.dph ? a.dph + q : nullptr;
+    const TC rdz = (TC)(1.0 / a.dz);
+    CC dn = L > 1 ? ld_d(L - 1) : mk<TC>(0, 0);
+    TC cn = L > 1 ? ld_c(L - 1) : (TC)0;
     for (int iz = L - 1; iz >= 1; --iz) {
-        const CC d = ld_d(iz);
-        const TC cp = ld_c(iz);
+        const CC d = dn;
+        const TC cp = cn;
+        if (iz > 1) {   // next level's operands ahead of this level's stores
+            dn = ld_d(iz - 1);
+            cn = ld_c(iz - 1);
+        }
         const CC p = mk<TC>(d.x - cp * pn.x, d.y - cp * pn.y);
-        if (dph) dph[S * (iz + 1)] = mk<TS>((TS)((pn.x - p.x) / dz), (TS)((pn.y - p.y) / dz));
+        if (dph) dph[S * (iz + 1)] = mk<TS>((TS)((pn.x - p.x) * rdz), (TS)((pn.y - p.y) * rdz));
         ph[S * iz] = mk<TS>((TS)p.x, (TS)p.y);
         pn = p;
     }
@@ -121,6 +136,24 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
     const CC p0 = mk<TC>(pn.x - dz * hz0.x, pn.y - dz * hz0.y);
     ph[0] = mk<TS>((TS)p0.x, (TS)p0.y);
     if (dph) dph[S] = mk<TS>((TS)((pn.x - p0.x) / dz), (TS)((pn.y - p0.y) / dz));
+}
+
+template <typename TS, typename TC, bool ISLAND>
+__global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
+{
+    tdma_column<TS, TC, ISLAND>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Mixed precision in one launch: the first nbi blocks solve the FP64 island columns (their
+// long sequential FP64 sweeps start first), the remaining blocks the FP32 bulk columns,
+// so the two overlap instead of running back to back.
+template <typename T>
+__global__ void __launch_bounds__(128) k_tdma_mixed(TdmaArgs<T> a, IslandArgs isl, int nbi)
+{
+    if ((int)blockIdx.x < nbi)
+        tdma_column<T, double, true>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    else
+        tdma_column<T, T, false>(a, isl, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
 }
 
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e)
@@ -135,9 +168,10 @@ template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cud
 template <typename T>
 void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s, cudaError_t &e)
 {
-    if (e != cudaSuccess || isl.n <= 0) return;
+    if (e != cudaSuccess) return;
     const int bs = 128;
-    k_tdma<T, double, true><<<(unsigned)((isl.n + bs - 1) / bs), bs, 0, s>>>(a, isl);
+    const int nbi = (int)((isl.n + bs - 1) / bs), nbb = (int)((a.S + bs - 1) / bs);
+    k_tdma_mixed<T><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi);
     e = cudaGetLastError();
 }
 
