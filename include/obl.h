@@ -200,6 +200,57 @@ int obl_step(obl_ctx *ctx, const obl_step_io *io);      /* host double*   */
 int obl_step_f32(obl_ctx *ctx, const obl_step_io *io);  /* host float*    */
 int obl_step_dev(obl_ctx *ctx, const obl_step_io *io);  /* device, storage type */
 
+/* ---- convec: the rotational convective term (108_convec.f90:11-202) ----
+   The padded-grid consumer of zero_padding / zero_unpadding: ddx/ddy and the level
+   differences of u,v,w, the vorticity, zero_padding of u,v,w and the vorticity,
+   cross_product on the 3/2 grid and zero_unpadding (single z-rank, no Stokes drift).
+   The wall-model dudz, dvdz at level 1 (wallstress_bottom, 104_wallstress.f90) are
+   taken equal to level 2; at level nz they are 0 (stress-free top, :249-253).
+   cx, cy, cz (ldx,nyt,0:nz): levels 1..nz-1 written.  Needs nzt >= 5. */
+int obl_convec(obl_ctx *ctx, const double *u, const double *v, const double *w,
+               double *cx, double *cy, double *cz);
+int obl_convec_dev(obl_ctx *ctx, const void *u, const void *v, const void *w,
+                   void *cx, void *cy, void *cz);
+
+/* ---- rollout step and its transpose (the adjoint) ----
+   step: u1 = P(u - dt*tadv1*convec(u)) on u,v,w (ldx,nyt,0:nz) in place, where P is
+   press_stag_array with divtz = 0, dpdz and project(): the explicit-Euler form of the
+   Adams-Bashforth update (103_flosol.f90:115,319-389) followed by the projection
+   (:168-188).  No counterpart entry point in the reference, which has no adjoint.
+   step_vjp: lu,lv,lw <- (d step / d state)^T (lu,lv,lw) at the state u,v,w; the
+   transposed pressure solve is the same solve (symmetric bands), the transposed 3/2
+   rule is the opposite transform, the convec fields are recomputed from the state.
+   Only the Neumann-top mode (OBL_TOP_NEUMANN); OBL_ERR_UNSUPPORTED otherwise. */
+int obl_rollout_step(obl_ctx *ctx, double *u, double *v, double *w);
+int obl_rollout_step_dev(obl_ctx *ctx, void *u, void *v, void *w);
+int obl_rollout_step_vjp(obl_ctx *ctx, const double *u, const double *v, const double *w,
+                         double *lu, double *lv, double *lw);
+int obl_rollout_step_vjp_dev(obl_ctx *ctx, const void *u, const void *v, const void *w,
+                             void *lu, void *lv, void *lw);
+
+/* ---- kinetic-energy objective (energy, 103_flosol.f90) ----
+   *J = sum over x < nxt, all y and the levels jz = 1..nz-1 whose uvp height
+   (jz-0.5)*dz*z_i (012_io.f90:295, in the units of lz_tot) lies in (z_lo, z_hi) of
+   0.5*(u^2 + v^2 + (0.5*(w(jz)+w(jz+1)))^2), accumulated in FP64 in a fixed order.
+   lu,lv,lw: NULL, or (ldx,nyt,0:nz) outputs receiving dJ/d(u,v,w). */
+int obl_ke_band(obl_ctx *ctx, const double *u, const double *v, const double *w,
+                double z_lo, double z_hi, double *J, double *lu, double *lv, double *lw);
+int obl_ke_band_dev(obl_ctx *ctx, const void *u, const void *v, const void *w,
+                    double z_lo, double z_hi, double *J, void *lu, void *lv, void *lw);
+
+/* ---- rollout gradient ----
+   nsteps rollout steps from u0,v0,w0 with the state of every step checkpointed on the
+   device, *J = ke band objective of the final state, and, when gu is not NULL, the
+   reverse sweep of step_vjp (each step's convec fields recomputed from its
+   checkpoint): gu,gv,gw = dJ/d(u0,v0,w0), x < nxt meaningful.  *J is a host double in
+   both variants. */
+int obl_rollout_grad(obl_ctx *ctx, int nsteps, const double *u0, const double *v0,
+                     const double *w0, double z_lo, double z_hi, double *J,
+                     double *gu, double *gv, double *gw);
+int obl_rollout_grad_dev(obl_ctx *ctx, int nsteps, const void *u0, const void *v0,
+                         const void *w0, double z_lo, double z_hi, double *J,
+                         void *gu, void *gv, void *gw);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,46 @@ int orc_step(const orc_grid *g, int npz, double *u, double *v, double *w,
              const double *theta, double *const d[8], double *const big[4],
              double *p, double *const dp[3]);
 
+/* ---- rollout problem of the adjoint (obl_oracle_adj.c) ---- */
+/* Rotational convective term of convec + cross_product (108_convec.f90:11-202), single
+   rank (coordz == 0 == npz-1), Stokes drift off (ust = vst = 0).  dudz, dvdz at level 1
+   (set by wallstress_bottom in the reference) are taken equal to level 2; at level nz they
+   are 0, the stress-free top of wallstress_top (104_wallstress.f90:249-253).
+   cx, cy, cz (ldx,nyt,0:nz) are written on levels 1..nz-1, x < nxt. */
+void orc_convec(const orc_grid *g, const double *u, const double *v, const double *w,
+                double *cx, double *cy, double *cz);
+
+/* P: press_stag_array with divtz = 0 in the Neumann-top (npz >= 2) mode, flosol's dpdz
+   and project(), in place.  Needs (nzt-1) even. */
+int orc_projection(const orc_grid *g, double *u, double *v, double *w);
+
+/* One rollout step u1 = P(u - dt*tadv1*convec(u)), u,v,w in place. */
+int orc_rollout_step(const orc_grid *g, double *u, double *v, double *w);
+
+/* J = sum over x < nxt, all y and the levels 1..nz-1 whose uvp height (jz-0.5)*dz*z_i
+   lies in (z_lo, z_hi) of ke = 0.5*(u^2 + v^2 + (0.5*(w(jz)+w(jz+1)))^2)
+   (energy, 103_flosol.f90).  If lu is not NULL, lu/lv/lw receive dJ/d(u,v,w). */
+double orc_ke_band(const orc_grid *g, const double *u, const double *v, const double *w,
+                   double z_lo, double z_hi, double *lu, double *lv, double *lw);
+
+/* Transposes, written as explicit transposed operators:
+   orc_projection_vjp: lambda <- P^T lambda, in place;
+   orc_convec_vjp: l(u,v,w) += (d convec / d(u,v,w))^T l(cx,cy,cz) at the state u,v,w;
+   orc_rollout_step_vjp: lambda <- (d step / d state)^T lambda at the state u,v,w. */
+int orc_projection_vjp(const orc_grid *g, double *lu, double *lv, double *lw);
+void orc_convec_vjp(const orc_grid *g, const double *u, const double *v, const double *w,
+                    const double *lcx, const double *lcy, const double *lcz,
+                    double *lu, double *lv, double *lw);
+int orc_rollout_step_vjp(const orc_grid *g, const double *u, const double *v, const double *w,
+                         double *lu, double *lv, double *lw);
+
+/* nsteps rollout steps from (u0,v0,w0) with a checkpoint of every step's state, J of
+   the final state, and (when gu is not NULL) dJ/d(u0,v0,w0) by the reverse sweep.
+   Returns nonzero on a bad size. */
+int orc_rollout_grad(const orc_grid *g, int nsteps, const double *u0, const double *v0,
+                     const double *w0, double z_lo, double z_hi, double *J,
+                     double *gu, double *gv, double *gw);
+
 /* threads used by the OpenMP loops (0 = leave the OpenMP default) */
 void orc_set_threads(int n);
 int  orc_get_threads(void);

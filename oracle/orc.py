@@ -73,6 +73,14 @@ def lib():
             "orc_dpdz": (None, [G, P, P]),
             "orc_project": (None, [G, P, P, P, P, P, P]),
             "orc_step": (I, [G, I, P, P, P, P, P, P, P, P]),
+            "orc_convec": (None, [G, P, P, P, P, P, P]),
+            "orc_projection": (I, [G, P, P, P]),
+            "orc_rollout_step": (I, [G, P, P, P]),
+            "orc_ke_band": (ctypes.c_double, [G, P, P, P, ctypes.c_double, ctypes.c_double, P, P, P]),
+            "orc_projection_vjp": (I, [G, P, P, P]),
+            "orc_convec_vjp": (None, [G, P, P, P, P, P, P, P, P, P]),
+            "orc_rollout_step_vjp": (I, [G, P, P, P, P, P, P]),
+            "orc_rollout_grad": (I, [G, I, P, P, P, ctypes.c_double, ctypes.c_double, P, P, P, P]),
             "orc_set_threads": (None, [I]),
             "orc_get_threads": (I, []),
         }
@@ -249,3 +257,65 @@ class Grid:
         if rc:
             raise ValueError("orc_step failed")
         return dict(u=u, v=v, w=w, d=d, big=big, p=p, dpdx=dp[0], dpdy=dp[1], dpdz=dp[2])
+
+    # --- rollout problem of the adjoint (obl_oracle_adj.c) ---
+    def _copies(self, *arrs):
+        return [np.array(a, dtype=np.float64, order="F", copy=True) for a in arrs]
+
+    def convec(self, u, v, w):
+        u, v, w = self._copies(u, v, w)
+        cx, cy, cz = self.field(), self.field(), self.field()
+        lib().orc_convec(self.ref, _p(u), _p(v), _p(w), _p(cx), _p(cy), _p(cz))
+        return cx, cy, cz
+
+    def projection(self, u, v, w):
+        u, v, w = self._copies(u, v, w)
+        if lib().orc_projection(self.ref, _p(u), _p(v), _p(w)):
+            raise ValueError("projection: (nzt-1) must be even")
+        return u, v, w
+
+    def rollout_step(self, u, v, w):
+        u, v, w = self._copies(u, v, w)
+        if lib().orc_rollout_step(self.ref, _p(u), _p(v), _p(w)):
+            raise ValueError("rollout_step: bad size")
+        return u, v, w
+
+    def ke_band(self, u, v, w, z_lo, z_hi, grad=False):
+        u, v, w = self._copies(u, v, w)
+        if grad:
+            lu, lv, lw = self.field(), self.field(), self.field()
+            J = lib().orc_ke_band(self.ref, _p(u), _p(v), _p(w), float(z_lo), float(z_hi),
+                                  _p(lu), _p(lv), _p(lw))
+            return J, (lu, lv, lw)
+        return lib().orc_ke_band(self.ref, _p(u), _p(v), _p(w), float(z_lo), float(z_hi),
+                                 None, None, None)
+
+    def projection_vjp(self, lu, lv, lw):
+        lu, lv, lw = self._copies(lu, lv, lw)
+        if lib().orc_projection_vjp(self.ref, _p(lu), _p(lv), _p(lw)):
+            raise ValueError("projection_vjp: bad size")
+        return lu, lv, lw
+
+    def convec_vjp(self, u, v, w, lcx, lcy, lcz):
+        u, v, w, lcx, lcy, lcz = self._copies(u, v, w, lcx, lcy, lcz)
+        lu, lv, lw = self.field(), self.field(), self.field()
+        lib().orc_convec_vjp(self.ref, _p(u), _p(v), _p(w), _p(lcx), _p(lcy), _p(lcz),
+                             _p(lu), _p(lv), _p(lw))
+        return lu, lv, lw
+
+    def rollout_step_vjp(self, u, v, w, lu, lv, lw):
+        u, v, w, lu, lv, lw = self._copies(u, v, w, lu, lv, lw)
+        if lib().orc_rollout_step_vjp(self.ref, _p(u), _p(v), _p(w), _p(lu), _p(lv), _p(lw)):
+            raise ValueError("rollout_step_vjp: bad size")
+        return lu, lv, lw
+
+    def rollout_grad(self, nsteps, u, v, w, z_lo, z_hi, grad=True):
+        u, v, w = self._copies(u, v, w)
+        J = ctypes.c_double(0.0)
+        g = [self.field() for _ in range(3)] if grad else [None, None, None]
+        P = [(_p(a) if a is not None else None) for a in g]
+        rc = lib().orc_rollout_grad(self.ref, int(nsteps), _p(u), _p(v), _p(w), float(z_lo),
+                                    float(z_hi), ctypes.byref(J), *P)
+        if rc:
+            raise ValueError("rollout_grad: bad size")
+        return (J.value, tuple(g)) if grad else J.value

@@ -42,6 +42,9 @@ EXPORTS = [
     "obl_press_stag_array", "obl_press_stag_array_dev",
     "obl_dpdz", "obl_dpdz_dev", "obl_project", "obl_project_dev",
     "obl_step", "obl_step_f32", "obl_step_dev",
+    "obl_convec", "obl_convec_dev", "obl_rollout_step", "obl_rollout_step_dev",
+    "obl_rollout_step_vjp", "obl_rollout_step_vjp_dev", "obl_ke_band", "obl_ke_band_dev",
+    "obl_rollout_grad", "obl_rollout_grad_dev",
 ]
 
 
@@ -92,6 +95,7 @@ def load_library(path=LIB_PATH):
         raise OblError(f"{path} is missing: build it with `python -m overlappingbls_b200.build`")
     L = ctypes.CDLL(path)
     P, I, C = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char)
+    D, DP = ctypes.c_double, ctypes.POINTER(ctypes.c_double)
     ctx = ctypes.c_void_p
     sig = {
         "obl_ctx_create": [ctypes.POINTER(Grid), ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)],
@@ -117,6 +121,14 @@ def load_library(path=LIB_PATH):
         "obl_project": [ctx, P, P, P, P, P, P], "obl_project_dev": [ctx, P, P, P, P, P, P],
         "obl_step": [ctx, ctypes.POINTER(StepIO)], "obl_step_f32": [ctx, ctypes.POINTER(StepIO)],
         "obl_step_dev": [ctx, ctypes.POINTER(StepIO)],
+        "obl_convec": [ctx, P, P, P, P, P, P], "obl_convec_dev": [ctx, P, P, P, P, P, P],
+        "obl_rollout_step": [ctx, P, P, P], "obl_rollout_step_dev": [ctx, P, P, P],
+        "obl_rollout_step_vjp": [ctx, P, P, P, P, P, P],
+        "obl_rollout_step_vjp_dev": [ctx, P, P, P, P, P, P],
+        "obl_ke_band": [ctx, P, P, P, D, D, DP, P, P, P],
+        "obl_ke_band_dev": [ctx, P, P, P, D, D, DP, P, P, P],
+        "obl_rollout_grad": [ctx, I, P, P, P, D, D, DP, P, P, P],
+        "obl_rollout_grad_dev": [ctx, I, P, P, P, D, D, DP, P, P, P],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -347,3 +359,58 @@ class Context:
             io.dp[i] = dp[i]
         io.divtz_bot, io.divtz_top = divtz_bot, divtz_top
         self._check(self._lib.obl_step_dev(self._h, ctypes.byref(io)), "step_dev")
+
+    # ---- rollout problem of the adjoint (host arrays, float64) ----
+    def convec(self, cx, cy, cz, u, v, w):
+        """convec(cx, cy, cz) of 108_convec.f90 at the state u, v, w (levels 1..nz-1)."""
+        self._check(self._lib.obl_convec(self._h, _ptr(u), _ptr(v), _ptr(w), _ptr(cx), _ptr(cy),
+                                         _ptr(cz)), "convec")
+
+    def rollout_step(self, u, v, w):
+        """u1 = P(u - dt*tadv1*convec(u)), in place."""
+        self._check(self._lib.obl_rollout_step(self._h, _ptr(u), _ptr(v), _ptr(w)), "rollout_step")
+
+    def rollout_step_vjp(self, u, v, w, lu, lv, lw):
+        """lu, lv, lw <- (d step / d state)^T (lu, lv, lw) at the state u, v, w, in place."""
+        self._check(self._lib.obl_rollout_step_vjp(self._h, _ptr(u), _ptr(v), _ptr(w), _ptr(lu),
+                                                   _ptr(lv), _ptr(lw)), "rollout_step_vjp")
+
+    def ke_band(self, u, v, w, z_lo, z_hi, lu=None, lv=None, lw=None):
+        J = ctypes.c_double(0.0)
+        self._check(self._lib.obl_ke_band(self._h, _ptr(u), _ptr(v), _ptr(w), float(z_lo),
+                                          float(z_hi), ctypes.byref(J), _ptr(lu), _ptr(lv),
+                                          _ptr(lw)), "ke_band")
+        return J.value
+
+    def rollout_grad(self, nsteps, u0, v0, w0, z_lo, z_hi, gu=None, gv=None, gw=None):
+        """J of the state after nsteps rollout steps; gu, gv, gw (optional outputs)
+        receive dJ/d(u0, v0, w0)."""
+        J = ctypes.c_double(0.0)
+        self._check(self._lib.obl_rollout_grad(self._h, int(nsteps), _ptr(u0), _ptr(v0), _ptr(w0),
+                                               float(z_lo), float(z_hi), ctypes.byref(J), _ptr(gu),
+                                               _ptr(gv), _ptr(gw)), "rollout_grad")
+        return J.value
+
+    # ---- the same on device pointers (storage type) ----
+    def convec_dev(self, cx, cy, cz, u, v, w):
+        self._check(self._lib.obl_convec_dev(self._h, u, v, w, cx, cy, cz), "convec_dev")
+
+    def rollout_step_dev(self, u, v, w):
+        self._check(self._lib.obl_rollout_step_dev(self._h, u, v, w), "rollout_step_dev")
+
+    def rollout_step_vjp_dev(self, u, v, w, lu, lv, lw):
+        self._check(self._lib.obl_rollout_step_vjp_dev(self._h, u, v, w, lu, lv, lw),
+                    "rollout_step_vjp_dev")
+
+    def ke_band_dev(self, u, v, w, z_lo, z_hi, lu=None, lv=None, lw=None):
+        J = ctypes.c_double(0.0)
+        self._check(self._lib.obl_ke_band_dev(self._h, u, v, w, float(z_lo), float(z_hi),
+                                              ctypes.byref(J), lu, lv, lw), "ke_band_dev")
+        return J.value
+
+    def rollout_grad_dev(self, nsteps, u0, v0, w0, z_lo, z_hi, gu=None, gv=None, gw=None):
+        J = ctypes.c_double(0.0)
+        self._check(self._lib.obl_rollout_grad_dev(self._h, int(nsteps), u0, v0, w0, float(z_lo),
+                                                   float(z_hi), ctypes.byref(J), gu, gv, gw),
+                    "rollout_grad_dev")
+        return J.value

@@ -15,6 +15,7 @@
 #include "lines.cuh"
 #include "press.cuh"
 #include "fused.cuh"
+#include "convec.cuh"
 
 using namespace obl;
 
@@ -53,6 +54,12 @@ struct obl_ctx {
     DevBuf isl_c, isl_d;
     DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
     DevBuf fscr;               // cluster scratch slots of the fused forward kernel
+    // rollout problem of the adjoint: small (ldx,nyt,0:nz) and padded work fields, the
+    // per-step state checkpoints and the objective's partial sums
+    DevBuf rw_small[18];
+    DevBuf rw_big[15];
+    DevBuf ckpt;
+    DevBuf ke;
     // tuning parameters (obl_set_param)
     long long param_fused = 0;          // use the cluster-fused kernels in obl_step
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
@@ -255,8 +262,10 @@ template <typename T> struct Ops {
     // rhs_ready: H_x, H_y, H_z at levels 1..L were already produced (by the fused
     // forward kernel); only the boundary planes H_z(0), H_z(nz) are transformed here.
     // proj: when given (with dpdz_out), the inverse is fused with project() on proj->u,v,w
+    // stress_free: overrides the context's ubc_stress_free for that project() (-1: keep)
     int press(const T *u, const T *v, const T *w, const T *dbot, const T *dtop, T *p, T *dpdx, T *dpdy,
-              T *dpdz_out = nullptr, bool rhs_ready = false, const obl_step_io *proj = nullptr)
+              T *dpdz_out = nullptr, bool rhs_ready = false, const obl_step_io *proj = nullptr,
+              int stress_free = -1)
     {
         const long long S = ctx->sp();
         const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
@@ -358,7 +367,7 @@ template <typename T> struct Ops {
             cudaError_t e = cudaSuccess;
             LaunchScope ls(ctx->rec, "project_bc", s());
             launch_project_bc<T>((T *)proj->u, (T *)proj->v, (T *)proj->w, ldx, ny, ctx->nz,
-                                 (int)ctx->opt.ubc_stress_free, s(), e);
+                                 stress_free < 0 ? (int)ctx->opt.ubc_stress_free : stress_free, s(), e);
             return chk(e, "project_bc");
         }
         // inverse transforms (:231-238): p at 0..L, dpdx/dpdy at 1..L; Hx/Hy/Hz are
@@ -508,6 +517,222 @@ template <typename T> struct Ops {
             return rc;
         return project((T *)io->u, (T *)io->v, (T *)io->w, (const T *)io->dp[0], (const T *)io->dp[1],
                        (const T *)io->dp[2]);
+    }
+
+    // ---- rollout problem of the adjoint ----
+    // small work fields (ldx,nyt,0:nz); in the transposed step the first ones are reused
+    enum { S_DUDY, S_DVDX, S_DWDX, S_DWDY, S_O1, S_O2, S_O3, S_CX, S_CY, S_CZ, S_P, S_DPDX, S_DPDY, S_DPDZ,
+           S_T1, S_T2, S_T3, S_T4, S_N };
+    // padded work fields (nxt2,nyt2,0:nz)
+    enum { B_U, B_V, B_W, B_O1, B_O2, B_O3, B_X, B_Y, B_Z, B_AU, B_AV, B_AW, B_A1, B_A2, B_A3, B_N };
+    T *rs(int i) { return (T *)ctx->rw_small[i].p; }
+    T *rb(int i) { return (T *)ctx->rw_big[i].p; }
+    int rollout_bufs()
+    {
+        int rc;
+        for (int i = 0; i < S_N; ++i)
+            if ((rc = ensure(ctx, ctx->rw_small[i], sizeof(T) * (size_t)ctx->field()))) return rc;
+        for (int i = 0; i < B_N; ++i)
+            if ((rc = ensure(ctx, ctx->rw_big[i], sizeof(T) * (size_t)ctx->big()))) return rc;
+        return OBL_OK;
+    }
+    BigSet<T> bigset() { return BigSet<T>{rb(B_U), rb(B_V), rb(B_W), rb(B_O1), rb(B_O2), rb(B_O3)}; }
+
+    // ddx/ddy of u, v, w, the vorticity and the six padded fields of convec
+    // (108_convec.f90:38-76, derivatives of 103_flosol.f90:30-37)
+    int convec_fields(const T *u, const T *v, const T *w)
+    {
+        const int nlev = ctx->nz + 1;
+        int rc;
+        if ((rc = ddy(rs(S_DUDY), u, nlev)) || (rc = ddx(rs(S_DVDX), v, nlev)) || (rc = ddx(rs(S_DWDX), w, nlev)) ||
+            (rc = ddy(rs(S_DWDY), w, nlev)))
+            return rc;
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "vort", s());
+            launch_vort<T>(u, v, rs(S_DUDY), rs(S_DVDX), rs(S_DWDX), rs(S_DWDY), rs(S_O1), rs(S_O2), rs(S_O3),
+                           ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
+            if ((rc = chk(e, "vort"))) return rc;
+        }
+        const T *src[6] = {u, v, w, rs(S_O1), rs(S_O2), rs(S_O3)};
+        for (int i = 0; i < 6; ++i)
+            if ((rc = pad(src[i], rb(B_U + i), nlev))) return rc;
+        return OBL_OK;
+    }
+
+    // convec (108_convec.f90:11-99): cx, cy, cz at levels 1..nz-1
+    int convec(const T *u, const T *v, const T *w, T *cx, T *cy, T *cz)
+    {
+        int rc;
+        if ((rc = rollout_bufs()) || (rc = convec_fields(u, v, w))) return rc;
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "cross", s());
+            launch_cross<T>(bigset(), rb(B_X), rb(B_Y), rb(B_Z), ctx->nxt2, ctx->nyt2, ctx->nz, s(), e);
+            if ((rc = chk(e, "cross"))) return rc;
+        }
+        const long long pl = ctx->plane(), plb = (long long)ctx->nxt2 * ctx->nyt2;
+        T *dst[3] = {cx, cy, cz};
+        for (int i = 0; i < 3; ++i)
+            if ((rc = unpad(rb(B_X + i) + plb, dst[i] + pl, ctx->nz - 1))) return rc;
+        return OBL_OK;
+    }
+
+    // P: press_stag_array (divtz = 0) + dpdz + project, in place
+    int projection(T *u, T *v, T *w, int stress_free)
+    {
+        if (int rc = rollout_bufs()) return rc;
+        obl_step_io io{};
+        io.u = u; io.v = v; io.w = w;
+        return press(u, v, w, nullptr, nullptr, rs(S_P), rs(S_DPDX), rs(S_DPDY), rs(S_DPDZ), false, &io,
+                     stress_free);
+    }
+
+    // u1 = P(u - dt*tadv1*convec(u)), in place
+    int rollout_step(T *u, T *v, T *w)
+    {
+        int rc;
+        // the work fields must exist before their addresses are taken below
+        if ((rc = rollout_bufs())) return rc;
+        if ((rc = convec(u, v, w, rs(S_CX), rs(S_CY), rs(S_CZ)))) return rc;
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "update", s());
+            launch_update<T>(u, v, w, rs(S_CX), rs(S_CY), rs(S_CZ), ctx->dt_nd * kTadv1, ctx->nxt, ctx->ldx,
+                             ctx->nyt, ctx->nz, s(), e);
+            if ((rc = chk(e, "update"))) return rc;
+        }
+        return projection(u, v, w, -1);
+    }
+
+    // lambda <- P^T lambda.  With the Neumann top the bands of every k^2 > 0 column are
+    // symmetric and the (0,0) column's transposed integration gives back the same mean
+    // removal, so P^T = (P without the stress-free copy) applied to M S^T lambda, where S^T
+    // is the transposed copy and M clears w(1), w(nz), plus the one entry P does not
+    // produce: the w(1) row, -dt*tadv1*p(1)/dz of that same solve.
+    int projection_vjp(T *lu, T *lv, T *lw)
+    {
+        int rc;
+        cudaError_t e = cudaSuccess;
+        {
+            LaunchScope ls(ctx->rec, "adj_project_bc", s());
+            launch_adj_project_bc<T>(lu, lv, lw, ctx->ldx, ctx->nyt, ctx->nz, (int)ctx->opt.ubc_stress_free, s(), e);
+            if ((rc = chk(e, "adj_project_bc"))) return rc;
+        }
+        if ((rc = projection(lu, lv, lw, 0))) return rc;
+        LaunchScope ls(ctx->rec, "adj_w1", s());
+        launch_adj_w1<T>(lw, rs(S_P), -(ctx->dt_nd * kTadv1) / ctx->dz, ctx->nxt, ctx->ldx, ctx->nyt, s(), e);
+        return chk(e, "adj_w1");
+    }
+
+    // lambda <- (d step / d state)^T lambda at the state (u, v, w)
+    int step_vjp(const T *u, const T *v, const T *w, T *lu, T *lv, T *lw)
+    {
+        const int nlev = ctx->nz + 1;
+        int rc;
+        if ((rc = rollout_bufs()) || (rc = projection_vjp(lu, lv, lw))) return rc;
+        // the state's convec fields (recomputed from the checkpoint), and the padded
+        // adjoints of cx, cy, cz: pad(lambda) scaled by -dt*tadv1 inside the transposed
+        // cross product (unpad^T = pad/2.25 and pad^T = 2.25*unpad cancel)
+        if ((rc = convec_fields(u, v, w))) return rc;
+        T *lam[3] = {lu, lv, lw};
+        for (int i = 0; i < 3; ++i)
+            if ((rc = pad(lam[i], rb(B_X + i), nlev))) return rc;
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "cross_adj", s());
+            CrossAdjOut<T> out{rb(B_AU), rb(B_AV), rb(B_AW), rb(B_A1), rb(B_A2), rb(B_A3)};
+            launch_cross_adj<T>(bigset(), rb(B_X), rb(B_Y), rb(B_Z), -ctx->dt_nd * kTadv1, out, ctx->nxt2,
+                                ctx->nyt2, ctx->nz, s(), e);
+            if ((rc = chk(e, "cross_adj"))) return rc;
+        }
+        // sU, sV, sW, s1, s2, s3 (unpadded adjoints) into the first six small fields
+        for (int i = 0; i < 6; ++i)
+            if ((rc = unpad(rb(B_AU + i), rs(S_DUDY + i), nlev))) return rc;
+        T *sU = rs(S_DUDY), *sV = rs(S_DVDX), *sW = rs(S_DWDX), *s1 = rs(S_DWDY), *s2 = rs(S_O1), *s3 = rs(S_O2);
+        T *q1 = rs(S_O3), *q2 = rs(S_CX);
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "adj_q", s());
+            launch_adj_q<T>(s1, s2, q1, q2, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, s(), e);
+            if ((rc = chk(e, "adj_q"))) return rc;
+        }
+        // ddx^T = -ddx, ddy^T = -ddy: the signs are applied in the combine kernel
+        if ((rc = ddy(rs(S_T1), s3, nlev)) || (rc = ddx(rs(S_T2), s3, nlev)) || (rc = ddx(rs(S_T3), q2, nlev)) ||
+            (rc = ddy(rs(S_T4), q1, nlev)))
+            return rc;
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "adj_combine", s());
+        AdjCombineArgs<T> a{lu, lv, lw, sU, sV, sW, s1, s2, rs(S_T1), rs(S_T2), rs(S_T3), rs(S_T4)};
+        launch_adj_combine<T>(a, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
+        return chk(e, "adj_combine");
+    }
+
+    // levels 1..nz-1 whose uvp height (k-0.5)*dz*z_i (012_io.f90:295) lies in (z_lo, z_hi)
+    void band(double z_lo, double z_hi, int &klo, int &khi)
+    {
+        klo = 1;
+        khi = 0;
+        bool any = false;
+        for (int k = 1; k <= ctx->nz - 1; ++k) {
+            const double z = ((double)k - 0.5) * ctx->dz * ctx->grid.z_i;
+            if (z > z_lo && z < z_hi) {
+                if (!any) klo = k;
+                khi = k;
+                any = true;
+            }
+        }
+    }
+
+    // J of energy (103_flosol.f90) over the band; seeds dJ/d(u,v,w) into lu, lv, lw if given
+    int ke_band(const T *u, const T *v, const T *w, double z_lo, double z_hi, double *J, T *lu, T *lv, T *lw)
+    {
+        int rc;
+        if ((rc = ensure(ctx, ctx->ke, sizeof(double) * (size_t)(ke_parts() + 1)))) return rc;
+        int klo, khi;
+        band(z_lo, z_hi, klo, khi);
+        double *part = (double *)ctx->ke.p;
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "ke_band", s());
+            ctx->rec.launches += 1;   // partial sums + their fixed-order sum
+            launch_ke_band<T>(u, v, w, lu, lv, lw, part, part + ke_parts(), ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz,
+                              klo, khi, s(), e);
+            if ((rc = chk(e, "ke_band"))) return rc;
+        }
+        if (J) {
+            CK(cudaMemcpyAsync(J, part + ke_parts(), sizeof(double), cudaMemcpyDeviceToHost, s()));
+            CK(cudaStreamSynchronize(s()));
+        }
+        return OBL_OK;
+    }
+
+    // nsteps rollout steps with a checkpoint of every step's state, J of the final state and,
+    // when gu is given, the reverse sweep of step_vjp from the checkpoints (each step's convec
+    // fields are recomputed from its checkpoint)
+    int rollout_grad(int nsteps, const T *u0, const T *v0, const T *w0, double z_lo, double z_hi, double *J,
+                     T *gu, T *gv, T *gw)
+    {
+        const size_t F = (size_t)ctx->field();
+        int rc;
+        if ((rc = ensure(ctx, ctx->ckpt, sizeof(T) * F * 3 * (size_t)(nsteps + 1)))) return rc;
+        T *ck = (T *)ctx->ckpt.p;
+        CK(cudaMemcpyAsync(ck, u0, sizeof(T) * F, cudaMemcpyDeviceToDevice, s()));
+        CK(cudaMemcpyAsync(ck + F, v0, sizeof(T) * F, cudaMemcpyDeviceToDevice, s()));
+        CK(cudaMemcpyAsync(ck + 2 * F, w0, sizeof(T) * F, cudaMemcpyDeviceToDevice, s()));
+        for (int n = 0; n < nsteps; ++n) {
+            T *a = ck + 3 * F * (size_t)n, *b = a + 3 * F;
+            CK(cudaMemcpyAsync(b, a, sizeof(T) * 3 * F, cudaMemcpyDeviceToDevice, s()));
+            if ((rc = rollout_step(b, b + F, b + 2 * F))) return rc;
+        }
+        T *last = ck + 3 * F * (size_t)nsteps;
+        if ((rc = ke_band(last, last + F, last + 2 * F, z_lo, z_hi, J, gu, gv, gw))) return rc;
+        if (!gu) return OBL_OK;
+        for (int n = nsteps - 1; n >= 0; --n) {
+            T *a = ck + 3 * F * (size_t)n;
+            if ((rc = step_vjp(a, a + F, a + 2 * F, gu, gv, gw))) return rc;
+        }
+        return OBL_OK;
     }
 };
 
@@ -728,6 +953,10 @@ int obl_ctx_destroy(obl_ctx *ctx)
     cudaFree(ctx->isl_d.p);
     cudaFree(ctx->tmp.p);
     cudaFree(ctx->fscr.p);
+    for (auto &b : ctx->rw_small) cudaFree(b.p);
+    for (auto &b : ctx->rw_big) cudaFree(b.p);
+    cudaFree(ctx->ckpt.p);
+    cudaFree(ctx->ke.p);
     for (auto &b : ctx->stage) cudaFree(b.p);
     for (auto &b : ctx->stage64) cudaFree(b.p);
     delete ctx;
@@ -1108,6 +1337,117 @@ int obl_step_f32(obl_ctx *ctx, const obl_step_io *io)
 {
     if (!ctx || !step_io_ok(io)) return OBL_ERR_ARG;
     return step_host<float>(ctx, io);
+}
+
+} // extern "C"
+
+// ============================================================================= rollout and its transpose
+static int rollout_check(obl_ctx *ctx, bool transpose)
+{
+    if (ctx->nz < 5) return fail(ctx, OBL_ERR_UNSUPPORTED, "rollout: needs nzt >= 5");
+    if (transpose && ctx->opt.top_bc != OBL_TOP_NEUMANN)
+        return fail(ctx, OBL_ERR_UNSUPPORTED, "rollout transpose: only the Neumann-top pressure mode (OBL_TOP_NEUMANN)");
+    return OBL_OK;
+}
+static const HArg kNoArg{nullptr, 0, false, false, 0, 0, 0, 0};
+
+extern "C" {
+
+int obl_convec_dev(obl_ctx *ctx, const void *u, const void *v, const void *w, void *cx, void *cy, void *cz)
+{
+    if (!ctx || !u || !v || !w || !cx || !cy || !cz) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, false)) return rc;
+    DEVCALL(ctx, return o.convec((const T *)u, (const T *)v, (const T *)w, (T *)cx, (T *)cy, (T *)cz););
+}
+int obl_rollout_step_dev(obl_ctx *ctx, void *u, void *v, void *w)
+{
+    if (!ctx || !u || !v || !w) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, false)) return rc;
+    DEVCALL(ctx, return o.rollout_step((T *)u, (T *)v, (T *)w););
+}
+int obl_rollout_step_vjp_dev(obl_ctx *ctx, const void *u, const void *v, const void *w, void *lu, void *lv,
+                             void *lw)
+{
+    if (!ctx || !u || !v || !w || !lu || !lv || !lw) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, true)) return rc;
+    DEVCALL(ctx, return o.step_vjp((const T *)u, (const T *)v, (const T *)w, (T *)lu, (T *)lv, (T *)lw););
+}
+int obl_ke_band_dev(obl_ctx *ctx, const void *u, const void *v, const void *w, double z_lo, double z_hi,
+                    double *J, void *lu, void *lv, void *lw)
+{
+    if (!ctx || !u || !v || !w || !J || (lu && (!lv || !lw))) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.ke_band((const T *)u, (const T *)v, (const T *)w, z_lo, z_hi, J, (T *)lu, (T *)lv,
+                                  (T *)lw););
+}
+int obl_rollout_grad_dev(obl_ctx *ctx, int nsteps, const void *u0, const void *v0, const void *w0, double z_lo,
+                         double z_hi, double *J, void *gu, void *gv, void *gw)
+{
+    if (!ctx || nsteps < 0 || !u0 || !v0 || !w0 || !J || (gu && (!gv || !gw))) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, gu != nullptr)) return rc;
+    DEVCALL(ctx, return o.rollout_grad(nsteps, (const T *)u0, (const T *)v0, (const T *)w0, z_lo, z_hi, J,
+                                       (T *)gu, (T *)gv, (T *)gw););
+}
+
+int obl_convec(obl_ctx *ctx, const double *u, const double *v, const double *w, double *cx, double *cy,
+               double *cz)
+{
+    if (!ctx || !u || !v || !w || !cx || !cy || !cz) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, false)) return rc;
+    const long long nf = ctx->field(), ny = ctx->nyt, nl = ctx->nz - 1;
+    std::vector<HArg> a{harg_in(u, nf), harg_in(v, nf), harg_in(w, nf),
+                        harg_out(cx, nf, false, ctx->ldx, ctx->nxt, ny, ny * nl),
+                        harg_out(cy, nf, false, ctx->ldx, ctx->nxt, ny, ny * nl),
+                        harg_out(cz, nf, false, ctx->ldx, ctx->nxt, ny, ny * nl)};
+    HOSTCALL(double, ctx, a,
+             return o.convec((const T *)d[0], (const T *)d[1], (const T *)d[2], (T *)d[3], (T *)d[4], (T *)d[5]););
+}
+int obl_rollout_step(obl_ctx *ctx, double *u, double *v, double *w)
+{
+    if (!ctx || !u || !v || !w) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, false)) return rc;
+    const long long nf = ctx->field();
+    std::vector<HArg> a{harg_out(u, nf, true, nf, nf, 0, 1), harg_out(v, nf, true, nf, nf, 0, 1),
+                        harg_out(w, nf, true, nf, nf, 0, 1)};
+    HOSTCALL(double, ctx, a, return o.rollout_step((T *)d[0], (T *)d[1], (T *)d[2]););
+}
+int obl_rollout_step_vjp(obl_ctx *ctx, const double *u, const double *v, const double *w, double *lu,
+                         double *lv, double *lw)
+{
+    if (!ctx || !u || !v || !w || !lu || !lv || !lw) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, true)) return rc;
+    const long long nf = ctx->field();
+    std::vector<HArg> a{harg_in(u, nf), harg_in(v, nf), harg_in(w, nf), harg_out(lu, nf, true, nf, nf, 0, 1),
+                        harg_out(lv, nf, true, nf, nf, 0, 1), harg_out(lw, nf, true, nf, nf, 0, 1)};
+    HOSTCALL(double, ctx, a,
+             return o.step_vjp((const T *)d[0], (const T *)d[1], (const T *)d[2], (T *)d[3], (T *)d[4],
+                               (T *)d[5]););
+}
+int obl_ke_band(obl_ctx *ctx, const double *u, const double *v, const double *w, double z_lo, double z_hi,
+                double *J, double *lu, double *lv, double *lw)
+{
+    if (!ctx || !u || !v || !w || !J || (lu && (!lv || !lw))) return OBL_ERR_ARG;
+    const long long nf = ctx->field();
+    std::vector<HArg> a{harg_in(u, nf), harg_in(v, nf), harg_in(w, nf),
+                        lu ? harg_out(lu, nf, false, nf, nf, 0, 1) : kNoArg,
+                        lu ? harg_out(lv, nf, false, nf, nf, 0, 1) : kNoArg,
+                        lu ? harg_out(lw, nf, false, nf, nf, 0, 1) : kNoArg};
+    HOSTCALL(double, ctx, a,
+             return o.ke_band((const T *)d[0], (const T *)d[1], (const T *)d[2], z_lo, z_hi, J, (T *)d[3],
+                              (T *)d[4], (T *)d[5]););
+}
+int obl_rollout_grad(obl_ctx *ctx, int nsteps, const double *u0, const double *v0, const double *w0,
+                     double z_lo, double z_hi, double *J, double *gu, double *gv, double *gw)
+{
+    if (!ctx || nsteps < 0 || !u0 || !v0 || !w0 || !J || (gu && (!gv || !gw))) return OBL_ERR_ARG;
+    if (int rc = rollout_check(ctx, gu != nullptr)) return rc;
+    const long long nf = ctx->field();
+    std::vector<HArg> a{harg_in(u0, nf), harg_in(v0, nf), harg_in(w0, nf),
+                        gu ? harg_out(gu, nf, false, nf, nf, 0, 1) : kNoArg,
+                        gu ? harg_out(gv, nf, false, nf, nf, 0, 1) : kNoArg,
+                        gu ? harg_out(gw, nf, false, nf, nf, 0, 1) : kNoArg};
+    HOSTCALL(double, ctx, a,
+             return o.rollout_grad(nsteps, (const T *)d[0], (const T *)d[1], (const T *)d[2], z_lo, z_hi, J,
+                                   (T *)d[3], (T *)d[4], (T *)d[5]););
 }
 
 } // extern "C"
