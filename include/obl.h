@@ -251,6 +251,46 @@ int obl_rollout_grad_dev(obl_ctx *ctx, int nsteps, const void *u0, const void *v
                          const void *w0, double z_lo, double z_hi, double *J,
                          void *gu, void *gv, void *gw);
 
+/* ---- ensemble: many independent instances through obl_step together ----
+   No counterpart in the reference (one run = one domain).  Each instance has its own
+   grid (and context: tables, work buffers); all share the options (precision, top
+   mode, device).  ios[i] are device buffers in the storage type, as for obl_step_dev.
+   Modes:
+     OBL_ENS_SEQUENTIAL  instance after instance on the ensemble's stream;
+     OBL_ENS_CONCURRENT  every instance on its own stream (fork/join);
+     OBL_ENS_PERSISTENT  one cooperative launch over the work list of all instances,
+                         dispatching on each unit's line lengths at run time (lengths
+                         32..256; divtz planes must be NULL).  A grid-barrier wait that
+                         gives up is reported by obl_ensemble_synchronize as
+                         OBL_ERR_TIMEOUT.
+     OBL_ENS_PERSISTENT_SPLIT  the same work list in three cooperative launches, one
+                         per register class (row passes at 2 CTAs/SM, column passes and
+                         the solve at 4).
+   obl_ensemble_capture_dev records one step for the given buffers into a CUDA graph
+   (after one uncaptured step that allocates every buffer); obl_ensemble_replay
+   launches it.  obl_ensemble_time_dev returns the CUDA-event time per step. */
+#define OBL_ENS_SEQUENTIAL 0
+#define OBL_ENS_CONCURRENT 1
+#define OBL_ENS_PERSISTENT 2
+#define OBL_ENS_PERSISTENT_SPLIT 3
+typedef struct obl_ensemble obl_ensemble;
+int obl_ensemble_create(const obl_grid *grids, int n, const obl_options *opt, obl_ensemble **out);
+int obl_ensemble_destroy(obl_ensemble *ens);
+int obl_ensemble_size(const obl_ensemble *ens);
+int obl_ensemble_context(obl_ensemble *ens, int i, obl_ctx **ctx);
+int obl_ensemble_set_mode(obl_ensemble *ens, int mode, int blocks_per_sm);
+int obl_ensemble_get_mode(const obl_ensemble *ens, int *mode, int *blocks_per_sm, int *blocks);
+int obl_ensemble_step_dev(obl_ensemble *ens, const obl_step_io *ios);
+int obl_ensemble_capture_dev(obl_ensemble *ens, const obl_step_io *ios);
+int obl_ensemble_replay(obl_ensemble *ens);
+int obl_ensemble_synchronize(obl_ensemble *ens);
+int obl_ensemble_time_dev(obl_ensemble *ens, const obl_step_io *ios, int use_graph, int warmup,
+                          int reps, double *ms_per_step);
+/* on != 0: the persistent kernel records the global timer at each phase boundary (CTA
+   0); ms (n >= 6 entries, may be NULL) receives the phases of the last persistent step */
+int obl_ensemble_phase_times(obl_ensemble *ens, int on, double *ms, int n);
+int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

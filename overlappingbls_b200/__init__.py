@@ -45,7 +45,12 @@ EXPORTS = [
     "obl_convec", "obl_convec_dev", "obl_rollout_step", "obl_rollout_step_dev",
     "obl_rollout_step_vjp", "obl_rollout_step_vjp_dev", "obl_ke_band", "obl_ke_band_dev",
     "obl_rollout_grad", "obl_rollout_grad_dev",
+    "obl_ensemble_create", "obl_ensemble_destroy", "obl_ensemble_size", "obl_ensemble_context",
+    "obl_ensemble_set_mode", "obl_ensemble_get_mode", "obl_ensemble_step_dev",
+    "obl_ensemble_capture_dev", "obl_ensemble_replay", "obl_ensemble_synchronize",
+    "obl_ensemble_time_dev", "obl_ensemble_phase_times", "obl_ensemble_last_error",
 ]
+ENS_MODES = {"sequential": 0, "concurrent": 1, "persistent": 2, "persistent_split": 3}
 
 
 class OblError(RuntimeError):
@@ -130,6 +135,19 @@ def load_library(path=LIB_PATH):
         "obl_rollout_grad": [ctx, I, P, P, P, D, D, DP, P, P, P],
         "obl_rollout_grad_dev": [ctx, I, P, P, P, D, D, DP, P, P, P],
     }
+    E, IP = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
+    sig.update({
+        "obl_ensemble_create": [ctypes.POINTER(Grid), I, ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)],
+        "obl_ensemble_destroy": [E], "obl_ensemble_size": [E],
+        "obl_ensemble_context": [E, I, ctypes.POINTER(ctypes.c_void_p)],
+        "obl_ensemble_set_mode": [E, I, I], "obl_ensemble_get_mode": [E, IP, IP, IP],
+        "obl_ensemble_step_dev": [E, ctypes.POINTER(StepIO)],
+        "obl_ensemble_capture_dev": [E, ctypes.POINTER(StepIO)], "obl_ensemble_replay": [E],
+        "obl_ensemble_synchronize": [E],
+        "obl_ensemble_time_dev": [E, ctypes.POINTER(StepIO), I, I, I, DP],
+        "obl_ensemble_phase_times": [E, I, DP, I],
+        "obl_ensemble_last_error": [E, ctypes.c_char_p, ctypes.c_size_t],
+    })
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
@@ -178,11 +196,27 @@ class Context:
             setattr(self, k, self.info[k])
         self.dtype = np.float64 if self.info["elem_bytes"] == 8 else np.float32
 
+    @classmethod
+    def _borrow(cls, handle, precision):
+        """A non-owning view of a context that another object (an Ensemble) owns."""
+        self = cls.__new__(cls)
+        self._lib = load_library()
+        self._h = ctypes.c_void_p(handle)
+        self._owned = False
+        self.precision = precision
+        inf = Info()
+        self._lib.obl_ctx_info(self._h, ctypes.byref(inf))
+        self.info = {k: getattr(inf, k) for k, _ in Info._fields_}
+        for k in ("nxt", "nyt", "nzt", "nz", "ldx", "lhx", "nxt2", "nyt2", "dz", "dt_nd"):
+            setattr(self, k, self.info[k])
+        self.dtype = np.float64 if self.info["elem_bytes"] == 8 else np.float32
+        return self
+
     # ---- lifecycle / plumbing ----
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self, "_owned", True):
             self._lib.obl_ctx_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -414,3 +448,111 @@ class Context:
                                                    float(z_hi), ctypes.byref(J), gu, gv, gw),
                     "rollout_grad_dev")
         return J.value
+
+
+def stepio_dev(u, v, w, theta, d, big, p, dp, divtz_bot=None, divtz_top=None):
+    """obl_step_io of integer device pointers."""
+    io = StepIO()
+    io.u, io.v, io.w, io.theta, io.p = u, v, w, theta, p
+    for i in range(8):
+        io.d[i] = d[i]
+    for i in range(4):
+        io.big[i] = big[i]
+    for i in range(3):
+        io.dp[i] = dp[i]
+    io.divtz_bot, io.divtz_top = divtz_bot, divtz_top
+    return io
+
+
+class Ensemble:
+    """Many independent instances (one grid each) advanced through obl_step together.
+
+    grids: list of dicts with nxt, nyt, nzt, lx_tot, ly_tot, lz_tot, z_i, dt (u_scale)."""
+
+    def __init__(self, grids, precision="mixed", top_bc="neumann", ubc_stress_free=False,
+                 fp64_k2_max=-1.0, device=0):
+        self._lib = load_library()
+        n = len(grids)
+        G = (Grid * n)()
+        for i, g in enumerate(grids):
+            G[i] = Grid(g["nxt"], g["nyt"], g["nzt"], g["lx_tot"], g["ly_tot"], g["lz_tot"], g["z_i"],
+                        g["dt"], g.get("u_scale", 1.0))
+        o = Options(PRECISION[precision], TOP_BC[top_bc], 1 if ubc_stress_free else 0,
+                    float(fp64_k2_max), int(device))
+        h = ctypes.c_void_p()
+        rc = self._lib.obl_ensemble_create(G, n, ctypes.byref(o), ctypes.byref(h))
+        if rc != OBL_OK:
+            raise OblError(f"obl_ensemble_create failed: {ERRORS.get(rc, rc)}")
+        self._h = h
+        self.n = n
+        self.precision = precision
+        self.contexts = []
+        for i in range(n):
+            c = ctypes.c_void_p()
+            self._check(self._lib.obl_ensemble_context(self._h, i, ctypes.byref(c)), "obl_ensemble_context")
+            self.contexts.append(Context._borrow(c.value, precision))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for c in self.contexts:
+                c._h = None
+            self._lib.obl_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != OBL_OK:
+            buf = ctypes.create_string_buffer(1024)
+            self._lib.obl_ensemble_last_error(self._h, buf, 1024)
+            raise OblError(f"{what}: {ERRORS.get(rc, rc)} {buf.value.decode()}")
+
+    def _ios(self, ios):
+        if len(ios) != self.n:
+            raise ValueError(f"expected {self.n} step buffers, got {len(ios)}")
+        arr = (StepIO * self.n)()
+        for i, io in enumerate(ios):
+            arr[i] = io
+        return arr
+
+    def set_mode(self, mode, blocks_per_sm=0):
+        self._check(self._lib.obl_ensemble_set_mode(self._h, ENS_MODES[mode], int(blocks_per_sm)),
+                    "obl_ensemble_set_mode")
+
+    def get_mode(self):
+        m, b, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.obl_ensemble_get_mode(self._h, ctypes.byref(m), ctypes.byref(b),
+                                                    ctypes.byref(nb)), "obl_ensemble_get_mode")
+        name = {v: k for k, v in ENS_MODES.items()}[m.value]
+        return name, b.value, nb.value
+
+    def step_dev(self, ios):
+        self._check(self._lib.obl_ensemble_step_dev(self._h, self._ios(ios)), "obl_ensemble_step_dev")
+
+    def capture_dev(self, ios):
+        self._check(self._lib.obl_ensemble_capture_dev(self._h, self._ios(ios)), "obl_ensemble_capture_dev")
+
+    def replay(self):
+        self._check(self._lib.obl_ensemble_replay(self._h), "obl_ensemble_replay")
+
+    def synchronize(self):
+        self._check(self._lib.obl_ensemble_synchronize(self._h), "obl_ensemble_synchronize")
+
+    def time_dev(self, ios, use_graph=True, warmup=3, reps=10):
+        ms = ctypes.c_double(0.0)
+        self._check(self._lib.obl_ensemble_time_dev(self._h, self._ios(ios), 1 if use_graph else 0,
+                                                    int(warmup), int(reps), ctypes.byref(ms)),
+                    "obl_ensemble_time_dev")
+        return ms.value
+
+    def phase_times(self, on=True):
+        """Turn the persistent kernel's phase stamps on/off; returns the 6 phase times (ms)
+        of the last persistent step."""
+        ms = (ctypes.c_double * 6)()
+        self._check(self._lib.obl_ensemble_phase_times(self._h, 1 if on else 0, ms, 6),
+                    "obl_ensemble_phase_times")
+        return list(ms)

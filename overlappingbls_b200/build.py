@@ -22,6 +22,10 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I" + INCLUDE,
          "--expt-relaxed-constexpr"]
+# per-file flags: the persistent ensemble kernel reads data other SMs wrote earlier in the
+# same launch, so its global loads default to the L2-only (.cg) cache policy
+FILE_FLAGS = {f: ["-Xptxas", "-dlcm=cg"] for f in
+              ("ensemble.cu", "ensemble_all.cu", "ensemble_part_rows.cu", "ensemble_part_mid.cu")}
 
 
 def _deps():
@@ -34,7 +38,7 @@ def _compile(src, force, hdr_mtime):
     if (not force and os.path.exists(obj)
             and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_mtime)):
         return obj, None
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, "$ " + " ".join(cmd) + "\n" + r.stdout + r.stderr

@@ -16,6 +16,7 @@
 #include "press.cuh"
 #include "fused.cuh"
 #include "convec.cuh"
+#include "ensemble.cuh"
 
 using namespace obl;
 
@@ -704,6 +705,87 @@ template <typename T> struct Ops {
             CK(cudaMemcpyAsync(J, part + ke_parts(), sizeof(double), cudaMemcpyDeviceToHost, s()));
             CK(cudaStreamSynchronize(s()));
         }
+        return OBL_OK;
+    }
+
+    // ---- ensemble: the arguments of this instance's units in the persistent kernel ----
+    // The same arguments fwd_lines and press(rhs_ready, proj) give the line kernels, except
+    // that the four x-padded intermediates (xpad4) are separate: all four fields' row units
+    // run in one phase.
+    int ens_inst(const obl_step_io *io, T *xpad4, EnsInst<T> &I)
+    {
+        const int nlev = ctx->nz + 1, nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        const int L = ctx->L, lhx = ctx->lhx, ldx = ctx->ldx;
+        const long long S = ctx->sp();
+        const size_t sb = sizeof(C2<T>) * (size_t)S * (ctx->nz + 1);
+        int rc;
+        for (int i = 0; i < 5; ++i)
+            if ((rc = ensure(ctx, ctx->spec[i], sb))) return rc;
+        if ((rc = ensure(ctx, ctx->cscr, sizeof(T) * (size_t)S * L))) return rc;
+        if (ctx->n_isl) {
+            if ((rc = ensure(ctx, ctx->isl_c, sizeof(double) * (size_t)ctx->n_isl * L))) return rc;
+            if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
+        }
+        C2<T> *H[3] = {(C2<T> *)ctx->spec[0].p, (C2<T> *)ctx->spec[1].p, (C2<T> *)ctx->spec[2].p};
+        C2<T> *ph = (C2<T> *)ctx->spec[3].p, *dph = (C2<T> *)ctx->spec[4].p;
+        const T *f[4] = {(const T *)io->u, (const T *)io->v, (const T *)io->w, (const T *)io->theta};
+        const double scp = ((1.0 / ((double)nx * ny)) / kTadv1) * (1.0 / ctx->dt_nd);
+        const int WB = ens_wb<T>();
+        I = EnsInst<T>{};
+        I.nx = nx; I.ny = ny; I.nlev = nlev; I.L = L;
+        for (int c = 0; c < 4; ++c) {
+            T *xb = xpad4 + (size_t)c * nx2 * ny * nlev;
+            RowsFwd3Args<T> &ra = I.rows[c];
+            ra.src = f[c]; ra.dfdx = (T *)io->d[2 * c]; ra.xpad = xb; ra.H = c < 3 ? H[c] : nullptr;
+            ra.npairs = (long long)ny * nlev / 2; ra.ldx = ldx; ra.ny = ny; ra.L = L;
+            ra.sc_press = scp; ra.kx = ctx->d_kx;
+            ra.twF = twt<T>(ctx, nx, ROLE_FWD); ra.twB = twt<T>(ctx, nx, ROLE_BWD);
+            ra.twPB = twt<T>(ctx, nx, ROLE_PADBWD);
+            I.padc[c] = colargs(xb, nx2, (long long)nx2 * ny, io->big[c], nx2, (long long)nx2 * ny2, nx2, nlev,
+                                1.0 / ny, OP_PAD, ny);
+            I.ddyc[c] = colargs(f[c], ldx, ctx->plane(), io->d[2 * c + 1], ldx, ctx->plane(), nx, nlev, 1.0 / ny,
+                                OP_DERIV, ny);
+            I.ddyc[c].ktab = ctx->d_ky1;
+            if (c < 3) {
+                I.fwdc[c] = colargs(H[c] + S, lhx, S, H[c] + S, lhx, S, lhx, L, 1.0, OP_FWD, ny);
+                I.fwdc[c].zero_nyq = 1;
+            }
+        }
+        I.rows_units = EnsGeoHost<T>::rows_units(nx, I.rows[0].npairs);
+        I.pad_nb = (nx2 / 2 + WB - 1) / WB;
+        I.ddy_nb = (nx / 2 + WB - 1) / WB;
+        I.fwd_nb = (lhx + WB - 1) / WB;
+        I.Hz = H[2];
+        I.S = S;
+        TdmaArgs<T> &ta = I.tdma;
+        ta.Hx = H[0]; ta.Hy = H[1]; ta.Hz = H[2]; ta.phat = ph; ta.cscr = (T *)ctx->cscr.p;
+        ta.kx = ctx->d_kx; ta.ky = ctx->d_ky2; ta.skip = ctx->n_isl ? ctx->d_skip : nullptr;
+        ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz; ta.dph = dph;
+        ta.neumann_top = ctx->opt.top_bc == OBL_TOP_NEUMANN;
+        I.isl = IslandArgs{ctx->d_isl, ctx->n_isl, (double *)ctx->isl_c.p, (double2 *)ctx->isl_d.p};
+        I.isl_units = (ctx->n_isl + 255) / 256;
+        I.bulk_units = (S + 255) / 256;
+        PinvColArgs<T> &pc = I.pc;
+        pc.ph = ph; pc.dph = dph; pc.Xp = H[2]; pc.Xdx = H[0]; pc.Xdy = H[1]; pc.Xdz = dph;
+        pc.S = S; pc.lhx = lhx; pc.kx = ctx->d_kx; pc.ky = ctx->d_ky2; pc.twB = twt<T>(ctx, ny, ROLE_BWD);
+        I.pc_nb = (lhx + WB - 1) / WB;
+        PinvRowArgs<T> &pr = I.pr;
+        pr.Xp = H[2]; pr.Xdx = H[0]; pr.Xdy = H[1]; pr.Xdz = dph;
+        pr.p = (T *)io->p; pr.dpdx = (T *)io->dp[0]; pr.dpdy = (T *)io->dp[1]; pr.dpdz = (T *)io->dp[2];
+        pr.u = (T *)io->u; pr.v = (T *)io->v; pr.w = (T *)io->w;
+        pr.npairs = (long long)ny * (L + 1) / 2;
+        pr.ldx = ldx; pr.ny = ny; pr.lhx = lhx;
+        pr.dt_tadv1 = (T)(ctx->dt_nd * kTadv1);
+        pr.twB = twt<T>(ctx, nx, ROLE_BWD);
+        I.pr_units = EnsGeoHost<T>::pinv_rows_units(nx, pr.npairs);
+        I.u = (T *)io->u; I.v = (T *)io->v; I.w = (T *)io->w;
+        I.ldx = ldx; I.nz = ctx->nz; I.stress_free = (int)ctx->opt.ubc_stress_free;
+        I.count[0] = 4 * I.rows_units;
+        I.count[1] = 4LL * I.pad_nb * nlev + 4LL * I.ddy_nb * nlev + 3LL * I.fwd_nb * L + 1;
+        I.count[2] = I.isl_units + I.bulk_units;
+        I.count[3] = (long long)I.pc_nb * (L + 1);
+        I.count[4] = I.pr_units;
+        I.count[5] = 1;
         return OBL_OK;
     }
 
@@ -1505,3 +1587,400 @@ extern "C" int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void 
         return o.pad_with_scratch((const T *)var, (T *)var_big, (T *)xb, nlev);
     });
 }
+
+// ============================================================================= ensemble
+// Many independent instances (each its own obl_ctx: grid, tables, work buffers) advanced
+// through the step together.  Modes:
+//   OBL_ENS_SEQUENTIAL  one instance after the other on the ensemble's stream;
+//   OBL_ENS_CONCURRENT  every instance on its own stream, forked from and joined back
+//                       to the ensemble's stream;
+//   OBL_ENS_PERSISTENT  one cooperative launch of the persistent kernel over the work
+//                       list of all instances (ensemble.cuh);
+//   OBL_ENS_PERSISTENT_SPLIT  the same work list in three cooperative launches, one per
+//                       register class (rows | columns + solve | x-inverse), so that the
+//                       light phases run at a higher occupancy.
+// Any mode can be captured once into a CUDA graph and replayed.
+struct obl_ensemble {
+    int dev = 0;
+    bool f64 = false;
+    cudaStream_t stream = nullptr;
+    std::vector<obl_ctx *> ctx;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> ev;          // [0] fork, [1..n] joins
+    int mode = OBL_ENS_PERSISTENT;
+    int bps = 0;                          // persistent CTAs per SM (0: all that fit)
+    bool phase_stamps = false;            // record the phase boundaries of the persistent kernel
+    // persistent mode
+    DevBuf xpad, inst, start, bar;
+    std::vector<long long> xoff;          // element offset of each instance's 4 x-padded planes
+    std::vector<obl_step_io> ios;         // the buffers the uploaded work list was built for
+    size_t smem[3] = {0, 0, 0};           // per launch of the persistent step
+    int blocks = 0;                       // 0: launch shape not built yet
+    int nblk[3] = {0, 0, 0};
+    // graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<obl_step_io> graph_ios;
+    int graph_mode = -1;
+    std::string err;
+};
+
+namespace {
+int efail(obl_ensemble *e, int code, const std::string &m)
+{
+    if (e) e->err = m;
+    return code;
+}
+#define ECK(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return efail(ens, OBL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool same_ios(const std::vector<obl_step_io> &a, const obl_step_io *b, int n)
+{
+    return (int)a.size() == n && std::memcmp(a.data(), b, sizeof(obl_step_io) * (size_t)n) == 0;
+}
+
+int ens_ctx_fail(obl_ensemble *ens, int i, int rc)
+{
+    return efail(ens, rc, "instance " + std::to_string(i) + ": " + ens->ctx[i]->err);
+}
+
+// builds and uploads the work list of the persistent kernel for these buffers
+// the launches of the persistent step: phase ranges and CTAs per SM of each
+struct EnsPart {
+    int pb, pe, minb;
+};
+static const EnsPart kEnsAll[1] = {{0, 6, 2}};
+static const EnsPart kEnsSplit[3] = {{0, 1, 2}, {1, 4, 4}, {4, 6, 2}};
+
+template <typename T> static int ens_part_bps(const EnsPart &p, size_t smem)
+{
+    if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, 2>::blocks_per_sm(smem);
+    if (p.pb == 0) return EnsKernel<T, 0, 1, 2>::blocks_per_sm(smem);
+    if (p.pb == 1) return EnsKernel<T, 1, 4, 4>::blocks_per_sm(smem);
+    return EnsKernel<T, 4, 6, 2>::blocks_per_sm(smem);
+}
+template <typename T> static cudaError_t ens_part_launch(const EnsPart &p, const EnsArgs<T> &a, int blocks, size_t smem,
+                                                        cudaStream_t s)
+{
+    if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, 2>::launch(a, blocks, smem, s);
+    if (p.pb == 0) return EnsKernel<T, 0, 1, 2>::launch(a, blocks, smem, s);
+    if (p.pb == 1) return EnsKernel<T, 1, 4, 4>::launch(a, blocks, smem, s);
+    return EnsKernel<T, 4, 6, 2>::launch(a, blocks, smem, s);
+}
+
+// builds and uploads the work list of the persistent kernel for these buffers
+template <typename T> int ens_prepare(obl_ensemble *ens, const obl_step_io *ios)
+{
+    const int n = (int)ens->ctx.size();
+    if (same_ios(ens->ios, ios, n) && ens->blocks > 0) return OBL_OK;
+    int rc;
+    std::vector<EnsInst<T>> h(n);
+    for (int i = 0; i < n; ++i) {
+        if (ios[i].divtz_bot || ios[i].divtz_top)
+            return efail(ens, OBL_ERR_UNSUPPORTED, "persistent ensemble: divtz planes must be NULL (zero)");
+        Ops<T> o{ens->ctx[i]};
+        if ((rc = o.ens_inst(&ios[i], (T *)ens->xpad.p + ens->xoff[i], h[i]))) return ens_ctx_fail(ens, i, rc);
+    }
+    std::vector<long long> st((size_t)kEnsPhases * (n + 1), 0);
+    for (int p = 0; p < kEnsPhases; ++p)
+        for (int i = 0; i < n; ++i) st[(size_t)p * (n + 1) + i + 1] = st[(size_t)p * (n + 1) + i] + h[i].count[p];
+    if ((rc = ensure(ens->ctx[0], ens->inst, sizeof(EnsInst<T>) * (size_t)n))) return ens_ctx_fail(ens, 0, rc);
+    if ((rc = ensure(ens->ctx[0], ens->start, sizeof(long long) * st.size()))) return ens_ctx_fail(ens, 0, rc);
+    ECK(cudaMemcpyAsync(ens->inst.p, h.data(), sizeof(EnsInst<T>) * (size_t)n, cudaMemcpyHostToDevice, ens->stream));
+    ECK(cudaMemcpyAsync(ens->start.p, st.data(), sizeof(long long) * st.size(), cudaMemcpyHostToDevice, ens->stream));
+    ECK(cudaStreamSynchronize(ens->stream));
+    int nsm = 0;
+    ECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ens->dev));
+    const bool split = ens->mode == OBL_ENS_PERSISTENT_SPLIT;
+    const EnsPart *parts = split ? kEnsSplit : kEnsAll;
+    for (int k = 0; k < (split ? 3 : 1); ++k) {
+        size_t smem = 0;
+        for (int i = 0; i < n; ++i)
+            smem = std::max(smem, EnsGeoHost<T>::smem(ens->ctx[i]->nxt, ens->ctx[i]->nyt, parts[k].pb, parts[k].pe));
+        int per = ens_part_bps<T>(parts[k], smem);
+        if (per <= 0) return efail(ens, OBL_ERR_UNSUPPORTED, "persistent ensemble kernel cannot be resident");
+        if (ens->bps > 0 && ens->bps < per) per = ens->bps;
+        ens->smem[k] = smem;
+        ens->nblk[k] = per * nsm;
+    }
+    ens->blocks = ens->nblk[0];
+    ens->ios.assign(ios, ios + n);
+    return OBL_OK;
+}
+
+template <typename T> int ens_step_t(obl_ensemble *ens, const obl_step_io *ios)
+{
+    const int n = (int)ens->ctx.size();
+    int rc;
+    if (ens->mode == OBL_ENS_PERSISTENT || ens->mode == OBL_ENS_PERSISTENT_SPLIT) {
+        if ((rc = ens_prepare<T>(ens, ios))) return rc;
+        EnsArgs<T> a{(const EnsInst<T> *)ens->inst.p, n, (const long long *)ens->start.p, (unsigned *)ens->bar.p,
+                     (int *)((unsigned *)ens->bar.p + 2),
+                     ens->phase_stamps ? (unsigned long long *)((unsigned *)ens->bar.p + 4) : nullptr};
+        const bool split = ens->mode == OBL_ENS_PERSISTENT_SPLIT;
+        for (int k = 0; k < (split ? 3 : 1); ++k) {
+            ECK(cudaMemsetAsync(ens->bar.p, 0, 2 * sizeof(unsigned), ens->stream));
+            LaunchScope ls(ens->ctx[0]->rec, "ensemble_persistent", ens->stream);
+            ECK(ens_part_launch<T>((split ? kEnsSplit : kEnsAll)[k], a, ens->nblk[k], ens->smem[k], ens->stream));
+        }
+        return OBL_OK;
+    }
+    const bool conc = ens->mode == OBL_ENS_CONCURRENT;
+    if (conc) ECK(cudaEventRecord(ens->ev[0], ens->stream));
+    for (int i = 0; i < n; ++i) {
+        obl_ctx *c = ens->ctx[i];
+        c->stream = conc ? ens->streams[i] : ens->stream;
+        if (conc) ECK(cudaStreamWaitEvent(c->stream, ens->ev[0], 0));
+        Ops<T> o{c};
+        if ((rc = o.step(&ios[i]))) return ens_ctx_fail(ens, i, rc);
+        if (conc) {
+            ECK(cudaEventRecord(ens->ev[1 + i], c->stream));
+            ECK(cudaStreamWaitEvent(ens->stream, ens->ev[1 + i], 0));
+        }
+    }
+    return OBL_OK;
+}
+
+int ens_step(obl_ensemble *ens, const obl_step_io *ios)
+{
+    return ens->f64 ? ens_step_t<double>(ens, ios) : ens_step_t<float>(ens, ios);
+}
+
+void ens_drop_graph(obl_ensemble *ens)
+{
+    if (ens->exec) cudaGraphExecDestroy(ens->exec);
+    if (ens->graph) cudaGraphDestroy(ens->graph);
+    ens->exec = nullptr;
+    ens->graph = nullptr;
+    ens->graph_ios.clear();
+    ens->graph_mode = -1;
+}
+} // namespace
+
+extern "C" {
+
+int obl_ensemble_create(const obl_grid *grids, int n, const obl_options *opt, obl_ensemble **out)
+{
+    if (!grids || n <= 0 || !out) return OBL_ERR_ARG;
+    *out = nullptr;
+    obl_ensemble *ens = new obl_ensemble();
+    ens->dev = opt ? opt->device : 0;
+    for (int i = 0; i < n; ++i) {
+        obl_ctx *c = nullptr;
+        int rc = obl_ctx_create(&grids[i], opt, &c);
+        if (rc) {
+            obl_ensemble_destroy(ens);
+            return rc;
+        }
+        ens->ctx.push_back(c);
+    }
+    ens->f64 = ens->ctx[0]->f64;
+    if (cudaSetDevice(ens->dev) != cudaSuccess || cudaStreamCreateWithFlags(&ens->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        obl_ensemble_destroy(ens);
+        return OBL_ERR_CUDA;
+    }
+    ens->streams.resize(n, nullptr);
+    ens->ev.resize(n + 1, nullptr);
+    bool ok = true;
+    for (int i = 0; i < n; ++i) {
+        ok = ok && cudaStreamCreateWithFlags(&ens->streams[i], cudaStreamNonBlocking) == cudaSuccess;
+        ens->ctx[i]->stream = ens->stream;
+    }
+    for (auto &e : ens->ev) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+    // persistent mode: four x-padded planes per instance, barrier words
+    size_t tot = 0;
+    for (int i = 0; i < n && ok; ++i) {
+        const obl_ctx *c = ens->ctx[i];
+        ens->xoff.push_back((long long)tot);
+        tot += (size_t)4 * c->nxt2 * c->nyt * (c->nz + 1);
+        if (!ens_length_supported(c->nxt) || !ens_length_supported(c->nyt)) ens->mode = OBL_ENS_SEQUENTIAL;
+    }
+    ok = ok && ensure(ens->ctx[0], ens->xpad, ens->ctx[0]->es() * tot) == OBL_OK;
+    // barrier words [0..1], error flag [2], phase stamps from [4] (8-byte aligned)
+    const size_t barb = 4 * sizeof(unsigned) + (kEnsPhases + 1) * sizeof(unsigned long long);
+    ok = ok && ensure(ens->ctx[0], ens->bar, barb) == OBL_OK;
+    ok = ok && cudaMemset(ens->bar.p, 0, barb) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        obl_ensemble_destroy(ens);
+        return OBL_ERR_NOMEM;
+    }
+    *out = ens;
+    return OBL_OK;
+}
+
+int obl_ensemble_destroy(obl_ensemble *ens)
+{
+    if (!ens) return OBL_OK;
+    cudaSetDevice(ens->dev);
+    if (ens->stream) cudaStreamSynchronize(ens->stream);
+    ens_drop_graph(ens);
+    for (auto s : ens->streams)
+        if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
+    for (auto e : ens->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto c : ens->ctx) {
+        c->stream = nullptr;
+        obl_ctx_destroy(c);
+    }
+    cudaFree(ens->xpad.p);
+    cudaFree(ens->inst.p);
+    cudaFree(ens->start.p);
+    cudaFree(ens->bar.p);
+    if (ens->stream) cudaStreamDestroy(ens->stream);
+    delete ens;
+    return OBL_OK;
+}
+
+int obl_ensemble_size(const obl_ensemble *ens) { return ens ? (int)ens->ctx.size() : -1; }
+
+int obl_ensemble_context(obl_ensemble *ens, int i, obl_ctx **ctx)
+{
+    if (!ens || !ctx || i < 0 || i >= (int)ens->ctx.size()) return OBL_ERR_ARG;
+    *ctx = ens->ctx[i];
+    return OBL_OK;
+}
+
+int obl_ensemble_set_mode(obl_ensemble *ens, int mode, int blocks_per_sm)
+{
+    if (!ens || mode < 0 || mode > 3 || blocks_per_sm < 0) return OBL_ERR_ARG;
+    if (mode == OBL_ENS_PERSISTENT || mode == OBL_ENS_PERSISTENT_SPLIT)
+        for (auto c : ens->ctx)
+            if (!ens_length_supported(c->nxt) || !ens_length_supported(c->nyt))
+                return efail(ens, OBL_ERR_UNSUPPORTED, "persistent ensemble: line length " +
+                                                           std::to_string(c->nxt) + "x" + std::to_string(c->nyt) +
+                                                           " has no persistent-kernel instantiation");
+    ens->mode = mode;
+    ens->bps = blocks_per_sm;
+    ens->blocks = 0;   // rebuild the launch shape on the next persistent step
+    ens->ios.clear();
+    for (auto c : ens->ctx) c->stream = ens->stream;
+    return OBL_OK;
+}
+
+int obl_ensemble_get_mode(const obl_ensemble *ens, int *mode, int *blocks_per_sm, int *blocks)
+{
+    if (!ens) return OBL_ERR_ARG;
+    if (mode) *mode = ens->mode;
+    if (blocks_per_sm) *blocks_per_sm = ens->bps;
+    if (blocks) *blocks = ens->blocks;
+    return OBL_OK;
+}
+
+int obl_ensemble_step_dev(obl_ensemble *ens, const obl_step_io *ios)
+{
+    if (!ens || !ios) return OBL_ERR_ARG;
+    for (size_t i = 0; i < ens->ctx.size(); ++i)
+        if (!step_io_ok(&ios[i])) return efail(ens, OBL_ERR_ARG, "instance " + std::to_string(i) + ": missing buffer");
+    if (cudaSetDevice(ens->dev) != cudaSuccess) return efail(ens, OBL_ERR_CUDA, "cudaSetDevice");
+    return ens_step(ens, ios);
+}
+
+int obl_ensemble_capture_dev(obl_ensemble *ens, const obl_step_io *ios)
+{
+    if (!ens || !ios) return OBL_ERR_ARG;
+    if (cudaSetDevice(ens->dev) != cudaSuccess) return efail(ens, OBL_ERR_CUDA, "cudaSetDevice");
+    const int n = (int)ens->ctx.size();
+    if (ens->exec && ens->graph_mode == ens->mode && same_ios(ens->graph_ios, ios, n)) return OBL_OK;
+    ens_drop_graph(ens);
+    // one uncaptured step first: every buffer is allocated and every table uploaded before
+    // capture starts (nothing may allocate while a stream is being captured)
+    int rc = obl_ensemble_step_dev(ens, ios);
+    if (rc) return rc;
+    ECK(cudaStreamSynchronize(ens->stream));
+    const bool timing = ens->ctx[0]->rec.timing;
+    for (auto c : ens->ctx) c->rec.timing = false;
+    ECK(cudaStreamBeginCapture(ens->stream, cudaStreamCaptureModeThreadLocal));
+    rc = ens_step(ens, ios);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(ens->stream, &g);
+    for (auto c : ens->ctx) c->rec.timing = timing;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    ECK(ce);
+    ens->graph = g;
+    ECK(cudaGraphInstantiate(&ens->exec, g, 0));
+    ens->graph_ios.assign(ios, ios + n);
+    ens->graph_mode = ens->mode;
+    return OBL_OK;
+}
+
+int obl_ensemble_replay(obl_ensemble *ens)
+{
+    if (!ens) return OBL_ERR_ARG;
+    if (!ens->exec) return efail(ens, OBL_ERR_ARG, "no captured graph");
+    if (cudaSetDevice(ens->dev) != cudaSuccess) return efail(ens, OBL_ERR_CUDA, "cudaSetDevice");
+    ECK(cudaGraphLaunch(ens->exec, ens->stream));
+    return OBL_OK;
+}
+
+int obl_ensemble_synchronize(obl_ensemble *ens)
+{
+    if (!ens) return OBL_ERR_ARG;
+    if (cudaSetDevice(ens->dev) != cudaSuccess) return efail(ens, OBL_ERR_CUDA, "cudaSetDevice");
+    ECK(cudaStreamSynchronize(ens->stream));
+    int flag = 0;
+    ECK(cudaMemcpy(&flag, (unsigned *)ens->bar.p + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        cudaMemset((unsigned *)ens->bar.p + 2, 0, sizeof(int));
+        return efail(ens, OBL_ERR_TIMEOUT, "persistent ensemble: a grid-barrier wait gave up");
+    }
+    return OBL_OK;
+}
+
+int obl_ensemble_time_dev(obl_ensemble *ens, const obl_step_io *ios, int use_graph, int warmup, int reps,
+                          double *ms_per_step)
+{
+    if (!ens || !ios || reps <= 0 || warmup < 0 || !ms_per_step) return OBL_ERR_ARG;
+    int rc;
+    if (use_graph && (rc = obl_ensemble_capture_dev(ens, ios))) return rc;
+    auto one = [&]() -> int { return use_graph ? obl_ensemble_replay(ens) : obl_ensemble_step_dev(ens, ios); };
+    for (int i = 0; i < warmup; ++i)
+        if ((rc = one())) return rc;
+    if ((rc = obl_ensemble_synchronize(ens))) return rc;
+    cudaEvent_t a, b;
+    ECK(cudaEventCreate(&a));
+    ECK(cudaEventCreate(&b));
+    ECK(cudaEventRecord(a, ens->stream));
+    for (int i = 0; i < reps && !rc; ++i) rc = one();
+    ECK(cudaEventRecord(b, ens->stream));
+    const int rs = obl_ensemble_synchronize(ens);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (rs) return rs;
+    *ms_per_step = (double)ms / reps;
+    return OBL_OK;
+}
+
+int obl_ensemble_phase_times(obl_ensemble *ens, int on, double *ms, int n)
+{
+    if (!ens) return OBL_ERR_ARG;
+    ens->phase_stamps = on != 0;
+    if (!ms) return OBL_OK;
+    if (n < kEnsPhases) return efail(ens, OBL_ERR_ARG, "phase_times: need room for every phase");
+    if (cudaSetDevice(ens->dev) != cudaSuccess) return efail(ens, OBL_ERR_CUDA, "cudaSetDevice");
+    unsigned long long t[kEnsPhases + 1];
+    ECK(cudaStreamSynchronize(ens->stream));
+    ECK(cudaMemcpy(t, (unsigned *)ens->bar.p + 4, sizeof t, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < kEnsPhases; ++i) ms[i] = (double)(t[i + 1] - t[i]) * 1e-6;
+    return OBL_OK;
+}
+
+int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n)
+{
+    if (!ens || !buf || n == 0) return OBL_ERR_ARG;
+    std::strncpy(buf, ens->err.c_str(), n - 1);
+    buf[n - 1] = 0;
+    return OBL_OK;
+}
+
+} // extern "C"

@@ -268,27 +268,23 @@ template <typename T> struct RowsFwd3Args {
     const C2<T> *twF, *twB, *twPB;
 };
 
+// Unit u of the multi-output row pass: warp w of the CTA takes the LPW row pairs from
+// (u*8 + w)*LPW.  Tables in shared memory; scr holds the 8*LPW per-line scratch lines.
+// Called by k_rows_fwd3 (grid-stride over units) and by the persistent ensemble kernel.
 template <typename T, int N>
-__global__ void __launch_bounds__(256, 2) k_rows_fwd3(RowsFwd3Args<T> a)
+__device__ __forceinline__ void rows_fwd3_unit(const RowsFwd3Args<T> &a, long long u, const C2<T> *twF,
+                                               const C2<T> *twB, const C2<T> *twPB, C2<T> *scr)
 {
     using C = C2<T>;
     using GG = FwdFusedGeo<T, N>;
     constexpr int N2 = GG::N2, LH = GG::LH, LPW = GG::LPW;
     constexpr int LL = GG::DD::LL;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twF = reinterpret_cast<C *>(smraw);
-    C *twB = twF + GG::TF;
-    C *twPB = twB + GG::TB;
-    C *scr = twPB + GG::TPB;
-    for (int i = threadIdx.x; i < GG::TF; i += blockDim.x) twF[i] = a.twF[i];
-    for (int i = threadIdx.x; i < GG::TB; i += blockDim.x) twB[i] = a.twB[i];
-    for (int i = threadIdx.x; i < GG::TPB; i += blockDim.x) twPB[i] = a.twPB[i];
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int g = lane / LL, t = lane % LL;
     C *line = scr + (warp * LPW + g) * scratch_len(N2);
-    for (long long base = ((long long)blockIdx.x * nw + warp) * LPW; base < a.npairs;
-         base += (long long)gridDim.x * nw * LPW) {
+    {
+        const long long base = (u * nw + warp) * LPW;
+        if (base >= a.npairs) return;
         const long long p = base + g;
         const bool act = p < a.npairs;
         const long long r0 = 2 * (act ? p : base);
@@ -303,6 +299,24 @@ __global__ void __launch_bounds__(256, 2) k_rows_fwd3(RowsFwd3Args<T> a)
         row_fwd_fused<T, N>(A, A + a.ldx, dA, dA + a.ldx, pA, pA + N2, sA, sB, act, spec, a.sc_press, a.kx,
                             twF, twB, twPB, line, t);
     }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_rows_fwd3(RowsFwd3Args<T> a)
+{
+    using C = C2<T>;
+    using GG = FwdFusedGeo<T, N>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + GG::TF;
+    C *twPB = twB + GG::TB;
+    C *scr = twPB + GG::TPB;
+    for (int i = threadIdx.x; i < GG::TF; i += blockDim.x) twF[i] = a.twF[i];
+    for (int i = threadIdx.x; i < GG::TB; i += blockDim.x) twB[i] = a.twB[i];
+    for (int i = threadIdx.x; i < GG::TPB; i += blockDim.x) twPB[i] = a.twPB[i];
+    __syncthreads();
+    const long long per = (long long)(blockDim.x >> 5) * GG::LPW;
+    for (long long u = blockIdx.x; u * per < a.npairs; u += gridDim.x) rows_fwd3_unit<T, N>(a, u, twF, twB, twPB, scr);
 }
 
 template <typename T> struct RowsFwd3Launch {
@@ -322,25 +336,20 @@ template <typename T> struct PinvColArgs {
     const C2<T> *twB;
 };
 
+// One CTA unit: line group bx of level z (twB in shared memory, buf = N*WB scratch).
 template <typename T, int N>
-__global__ void __launch_bounds__(256, 2) k_cols_pinv(PinvColArgs<T> a)
+__device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, int z, const C2<T> *twB, C2<T> *buf)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_INV>;
     using G = LmGeo<T>;
     constexpr int WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP_INV>::VR;
     constexpr int R0 = D::RB0, RL = D::RBL;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twB = reinterpret_cast<C *>(smraw);
-    C *buf = twB + D::TB;
-    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int line = lane % WB, t = lane / WB + (32 / WB) * warp;
-    const int gl = blockIdx.x * WB + line;
+    const int gl = bx * WB + line;
     const bool act = gl < a.lhx;
     const int glc = act ? gl : 0;
-    const int z = blockIdx.y;
     LineMinor<C, WB> sc{buf, line};
     using G0 = Geo<N, R0, LL>;
     using GL = Geo<N, RL, LL>;
@@ -397,6 +406,19 @@ __global__ void __launch_bounds__(256, 2) k_cols_pinv(PinvColArgs<T> a)
     store(a.Xdz, w);
 }
 
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_cols_pinv(PinvColArgs<T> a)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP_INV>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twB = reinterpret_cast<C *>(smraw);
+    C *buf = twB + D::TB;
+    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
+    __syncthreads();
+    pinv_cols_unit<T, N>(a, blockIdx.x, blockIdx.y, twB, buf);
+}
+
 // x-inverse of the four y-inverses and the projection (110_project.f90:16-40) in one
 // pass over the rows: p at levels 0..L, dpdx/dpdy/dpdz at 1..L (slot z-1), and
 // u,v (levels 1..L) and w (levels 2..L) += dt*(-tadv1*grad p).
@@ -410,18 +432,14 @@ template <typename T> struct PinvRowArgs {
     const C2<T> *twB;
 };
 
+// Unit u: warp w takes work item u*8 + w (twB in shared memory, scr = 8*LPW lines).
 template <typename T, int N>
-__global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
+__device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long long u, const C2<T> *twB, C2<T> *scr)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_INV>;
     constexpr int LL = D::LL, LPW = D::LPW, VR = D::VR, R0 = D::RB0, RL = D::RBL;
     constexpr int SL = scratch_len(N);
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twB = reinterpret_cast<C *>(smraw);
-    C *scr = twB + D::TB;
-    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int g = lane / LL, t = lane % LL;
     LineScratch<C> sc{scr + (warp * LPW + g) * SL};
@@ -432,14 +450,16 @@ __global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
     // work item wi: component q = wi % 4 (0: p; 1: dpdx and u; 2: dpdy and v; 3: dpdz and w)
     // of the LPW row pairs of group wi / 4.  Independent items keep many row transforms in
     // flight per SM instead of four dependent ones per warp.
-    for (long long wi = (long long)blockIdx.x * nw + warp; wi < 4 * ngroups; wi += (long long)gridDim.x * nw) {
+    {
+        const long long wi = u * nw + warp;
+        if (wi >= 4 * ngroups) return;
         const int q = (int)(wi % 4);
         const long long base = (wi / 4) * LPW;
         const long long pr = base + g;
         const bool act = pr < a.npairs;
         const long long r0 = 2 * (act ? pr : base);
         const int z = (int)((2 * base) / a.ny);            // warp-uniform level
-        if (q > 0 && z == 0) continue;                     // level 0 holds p only
+        if (q > 0 && z == 0) return;                       // level 0 holds p only
         const long long off = (r0 % a.ny) * a.ldx;
         const C *X = q == 0 ? a.Xp : q == 1 ? a.Xdx : q == 2 ? a.Xdy : a.Xdz;
         T *out = q == 0 ? a.p + pl * z + off : (q == 1 ? a.dpdx : q == 2 ? a.dpdy : a.dpdz) + pl * (z - 1) + off;
@@ -501,6 +521,21 @@ __global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
             }
         }
     }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256, 2) k_rows_pinv(PinvRowArgs<T> a)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP_INV>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twB = reinterpret_cast<C *>(smraw);
+    C *scr = twB + D::TB;
+    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
+    __syncthreads();
+    const long long ngroups = (a.npairs + D::LPW - 1) / D::LPW;
+    const long long nunits = (4 * ngroups + (blockDim.x >> 5) - 1) / (blockDim.x >> 5);
+    for (long long u = blockIdx.x; u < nunits; u += gridDim.x) pinv_rows_unit<T, N>(a, u, twB, scr);
 }
 template <typename T> struct PinvLaunch {
     static cudaError_t cols(int n, const PinvColArgs<T> &a, int nlev, cudaStream_t s);

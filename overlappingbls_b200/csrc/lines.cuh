@@ -520,28 +520,26 @@ template <typename T, int N, int OP> struct ColDerived {
     static constexpr int VR = rf > rb ? rf : rb;
 };
 
+// One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
+// tables twF/twB are already in shared memory; buf is the exchange scratch (NM*WB).
+// Called by k_cols2 (one unit per CTA) and by the persistent ensemble kernel.
 template <typename T, int N, int OP, bool REAL>
-__global__ void __launch_bounds__(256) k_cols2(ColArgs<T> a)
+__device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, const C2<T> *twF,
+                                           const C2<T> *twB, C2<T> *buf)
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
     using D = LineDerived<N, OP>;
     using G = LmGeo<T>;
     constexpr int NI = D::NI, NO = D::NO, WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP>::VR;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twF = reinterpret_cast<C *>(smraw);
-    C *twB = twF + D::TF;
-    C *buf = twB + D::TB;
-    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
-    __syncthreads();
-
+    (void)NI;
+    (void)twF;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int line = lane % WB, t = lane / WB + (32 / WB) * warp;
-    const int gl = blockIdx.x * WB + line;                 // global line index
+    const int gl = bx * WB + line;                         // global line index
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
     const bool act = gl < nlines;
     const int glc = act ? gl : 0;
-    const int z = blockIdx.y;
     // element i of this line: a complex value (a real column pair for REAL)
     const E *srcz = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane;
     E *dstz = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane;
@@ -646,6 +644,20 @@ __global__ void __launch_bounds__(256) k_cols2(ColArgs<T> a)
             }
         }
     }
+}
+
+template <typename T, int N, int OP, bool REAL>
+__global__ void __launch_bounds__(256) k_cols2(ColArgs<T> a)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *twF = reinterpret_cast<C *>(smraw);
+    C *twB = twF + D::TF;
+    C *buf = twB + D::TB;
+    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
+    __syncthreads();
+    cols2_unit<T, N, OP, REAL>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
 }
 
 // ----------------------------------------------------------------------------- launchers

@@ -28,6 +28,127 @@ struct IslandArgs {
     double2 *dscr;     // (n, L+1)
 };
 
+// One column's solve; t = the thread's index among the bulk columns or in the island list.
+template <typename TS, typename TC, bool ISLAND>
+__device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandArgs &isl, long long t)
+{
+    using CS = C2<TS>;
+    using CC = C2<TC>;
+    long long q;
+    if constexpr (ISLAND) {
+        if (t >= isl.n) return;
+        q = isl.cols[t];
+    } else {
+        if (t >= a.S) return;
+        q = t;
+        if (a.skip && a.skip[q]) return;
+    }
+    const long long S = a.S;
+    const int L = a.L;
+    const int ix = (int)(q % a.lhx), iy = (int)(q / a.lhx);
+    CS *ph = a.phat + q;
+
+    // Nyquist columns: p_hat = 0 at every level (:303-305, and the caller's zero fill)
+    if (ix == a.lhx - 1 || iy == a.nyt / 2) {
+        for (int z = 0; z <= L; ++z) ph[S * z] = mk<TS>(0, 0);
+        if (a.dph)
+            for (int z = 1; z <= L; ++z) a.dph[q + S * z] = mk<TS>(0, 0);
+        return;
+    }
+    const double kxd = a.kx[ix], kyd = a.ky[iy];
+    const double k2d = kxd * kxd + kyd * kyd;   // 002_fft.f90:167
+    const bool m00 = (k2d == 0.0);              // the (0,0) mean mode
+    const TC kx = (TC)kxd, ky = (TC)kyd, k2 = (TC)k2d;
+    const TC dz = (TC)a.dz, idz = (TC)(1.0 / a.dz), idz2 = (TC)(1.0 / (a.dz * a.dz));
+
+    auto ld = [&](const CS *p, int z) -> CC {
+        const CS v = p[q + S * z];
+        return mk<TC>((TC)v.x, (TC)v.y);
+    };
+    auto st_d = [&](int z, CC v) {
+        if constexpr (ISLAND) isl.dscr[t + (long long)isl.n * z] = make_double2(v.x, v.y);
+        else ph[S * z] = v;
+    };
+    auto ld_d = [&](int z) -> CC {
+        if constexpr (ISLAND) { const double2 v = isl.dscr[t + (long long)isl.n * z]; return mk<TC>(v.x, v.y); }
+        else return ph[S * z];
+    };
+    auto st_c = [&](int z, TC v) {
+        if constexpr (ISLAND) isl.cscr[t + (long long)isl.n * (z - 1)] = v;
+        else a.cscr[q + S * (z - 1)] = v;
+    };
+    auto ld_c = [&](int z) -> TC {
+        if constexpr (ISLAND) return isl.cscr[t + (long long)isl.n * (z - 1)];
+        else return a.cscr[q + S * (z - 1)];
+    };
+
+    // ---- forward elimination ----
+    // The RHS inputs of level iz+1 are loaded while level iz is eliminated (the loads are
+    // independent of the recurrence; issuing them ahead hides their latency).
+    const CC hz0 = ld(a.Hz, 0);     // RHS_col(0) = H_z(0) (:209)
+    CC hzc = ld(a.Hz, 1);
+    CC hzn = ld(a.Hz, 2);
+    CC hx = ld(a.Hx, 1), hy = ld(a.Hy, 1);
+    CC dprev = hz0;
+    TC cprev = 0;                   // coef_cp(0) = 0 on the bottom rank
+    for (int iz = 1; iz <= L; ++iz) {
+        const int izn = iz < L ? iz + 1 : iz;
+        const CC hx_n = ld(a.Hx, izn), hy_n = ld(a.Hy, izn), hz_n = ld(a.Hz, izn + 1);
+        TC am, bm, cm;
+        CC r;
+        if (!m00) {
+            const bool top = a.neumann_top && iz == L;
+            am = (iz == 1) ? (TC)0 : idz2;
+            bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (TC)2 * idz2);
+            cm = top ? (TC)0 : idz2;
+            const CC sxy = mk<TC>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
+            CC dh = csub(hzn, hzc);
+            if (iz == 1) dh = cadd(dh, hz0);
+            r = mk<TC>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+        } else {
+            am = (iz == 1) ? (TC)0 : -idz;
+            bm = idz;
+            cm = 0;
+            r = (iz == 1) ? mk<TC>(0, 0) : hzc;
+        }
+        const TC bp = bm - am * cprev;
+        const TC ibp = (TC)1 / bp;
+        const TC cp = cm * ibp;
+        const CC d = mk<TC>((r.x - am * dprev.x) * ibp, (r.y - am * dprev.y) * ibp);
+        st_c(iz, cp);
+        st_d(iz, d);
+        cprev = cp;
+        dprev = d;
+        hzc = hzn;
+        hzn = hz_n;
+        hx = hx_n;
+        hy = hy_n;
+    }
+    // ---- back substitution ----
+    CC pn = a.neumann_top ? dprev : mk<TC>(0, 0);   // p_hat(nz-1): solved row / forced 0
+    ph[S * L] = mk<TS>((TS)pn.x, (TS)pn.y);
+    C2<TS> *dph = a.dph ? a.dph + q : nullptr;
+    const TC rdz = (TC)(1.0 / a.dz);
+    CC dn = L > 1 ? ld_d(L - 1) : mk<TC>(0, 0);
+    TC cn = L > 1 ? ld_c(L - 1) : (TC)0;
+    for (int iz = L - 1; iz >= 1; --iz) {
+        const CC d = dn;
+        const TC cp = cn;
+        if (iz > 1) {   // next level's operands ahead of this level's stores
+            dn = ld_d(iz - 1);
+            cn = ld_c(iz - 1);
+        }
+        const CC p = mk<TC>(d.x - cp * pn.x, d.y - cp * pn.y);
+        if (dph) dph[S * (iz + 1)] = mk<TS>((TS)((pn.x - p.x) * rdz), (TS)((pn.y - p.y) * rdz));
+        ph[S * iz] = mk<TS>((TS)p.x, (TS)p.y);
+        pn = p;
+    }
+    // Neumann ghost level below the wall (:313-315)
+    const CC p0 = mk<TC>(pn.x - dz * hz0.x, pn.y - dz * hz0.y);
+    ph[0] = mk<TS>((TS)p0.x, (TS)p0.y);
+    if (dph) dph[S] = mk<TS>((TS)((pn.x - p0.x) / dz), (TS)((pn.y - p0.y) / dz));
+}
+
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e);
 template <typename T> void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl,
                                               cudaStream_t s, cudaError_t &e);

@@ -102,3 +102,18 @@ def make_fields(nxt, nyt, nzt, lz_tot=1000.0, z0=0.1, theta_grad=0.01, seed=2024
 # default physical constants of the benchmark workloads (dimensional)
 DOMAIN = dict(lx_tot=2 * np.pi * 1000.0, ly_tot=2 * np.pi * 1000.0, lz_tot=1000.0, z_i=1000.0,
               dt=0.5, u_scale=1.0)
+
+
+def ensemble_members(seed=2024):
+    """The 48 instances of the ensemble workload: 16 each at 96x96x64, 128x128x96 and
+    192x192x128 levels (nzt = levels + 1).  Per instance, from its own seeded stream: a
+    theta gradient ~ U[0, 0.03] K/m and a roughness length z0 log-uniform in [0.01, 1] m
+    (z0 replaces 0.1 m in the log law)."""
+    out = []
+    for b, (n, levels) in enumerate(((96, 64), (128, 96), (192, 128))):
+        for k in range(16):
+            i = 16 * b + k
+            r = uniform(int(_key(seed, 7, i)), 2)
+            out.append(dict(nxt=n, nyt=n, nzt=levels + 1, seed=seed + 1 + i,
+                            theta_grad=0.03 * float(r[0]), z0=10.0 ** (-2.0 + 2.0 * float(r[1]))))
+    return out
