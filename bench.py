@@ -9,8 +9,11 @@ dpdz and project -- obl_step_dev through the C ABI.  Mpts/s = nx*ny*(nzt-1)/t/1e
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Default workload: 512 x 512 x 256 levels, FP32-mixed (the headline configuration).
-Multi-GPU (torchrun): every rank advances its own instance (independent replicas,
-weak scaling, no data-path collective); the time is the max over ranks.
+Multi-GPU (torchrun), --mode slab (default): one domain of 512 x 512 x (256 N) levels split
+in z, each rank holding a 512 x 512 x 256-level slab (weak scaling); the step is the
+z-slab step of overlappingbls_b200.slab (partitioned pressure solve, two all-gathers over
+NCCL per step).  --mode replicas: every rank advances its own independent instance.  The
+time is the max over ranks.
 --impl reference times the FP64 CPU restatement of the reference path (the oracle)
 on the host cores, on a bounded sample of the same workload.
 """
@@ -112,7 +115,16 @@ def algorithmic_bytes(name, info, s):
         "pad_cols": (nx2 * ny + nx2 * ny2) * nlev * s,
         "press_fwd_rows": nx * ny * L * s + lhx * ny * L * c,
         "press_fwd_cols": 2 * lhx * ny * L * c,
-        "tdma": 4 * lhx * ny * L * c,
+        "tdma": 5 * lhx * ny * L * c,
+        "tdma_mixed": 5 * lhx * ny * L * c,
+        # one launch per field: field in, ddx and the x-padded rows out, and on u, v, w the
+        # RHS x-spectrum of levels 1..L out (mean over the 4 launches of a step)
+        "rows_fwd3": ((2 * nx + nx2) * ny * nlev * s * 4 + 3 * lhx * ny * L * c) / 4,
+        # p_hat (0..L) and the dpdz spectrum in; y-inverses of p, dpdx, dpdy, dpdz out
+        "pinv_cols": (2 * L + 1) * lhx * ny * c + (4 * L + 1) * lhx * ny * c,
+        # the four y-inverses and u, v, w in; p, dpdx, dpdy, dpdz and u, v, w out
+        "pinv_rows_project": (4 * L + 1) * lhx * ny * c + 3 * nx * ny * L * s + (4 * L + 1) * nx * ny * s
+                             + 3 * nx * ny * L * s,
     }
     return table.get(name)
 
@@ -120,7 +132,7 @@ def algorithmic_bytes(name, info, s):
 def run_ours(args, rank, local, world):
     import torch
     import overlappingbls_b200 as obl
-    from overlappingbls_b200 import fields
+    from overlappingbls_b200 import fields, slab
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -134,6 +146,9 @@ def run_ours(args, rank, local, world):
         # mixed-vs-FP64 error measures the computation rather than the input rounding
         f64 = {k: v.astype(np.float32).astype(np.float64) for k, v in f64.items()}
     stream = torch.cuda.current_stream(dev)
+    slab_mode = world > 1 and args.mode == "slab"
+    comm = slab.TorchComm() if slab_mode else None
+    slabs = {}
 
     def make_ctx(prec):
         c = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", device=local,
@@ -142,6 +157,8 @@ def run_ours(args, rank, local, world):
         for kv in args.param:
             k, v = kv.split("=")
             c.set_param(k, int(v))
+        if slab_mode:
+            slabs[id(c)] = slab.SlabStep(slab.LibBackend(c), rank, world, comm)
         return c
 
     def dev_set(ctx, dtype):
@@ -157,6 +174,12 @@ def run_ours(args, rank, local, world):
 
     def step(ctx, S):
         t, _, d, big, p, dp = S
+        if slab_mode:
+            io = obl.stepio_dev(t["u"].data_ptr(), t["v"].data_ptr(), t["w"].data_ptr(), t["theta"].data_ptr(),
+                                [x.data_ptr() for x in d], [x.data_ptr() for x in big], p.data_ptr(),
+                                [x.data_ptr() for x in dp])
+            slabs[id(ctx)].step(io)
+            return
         ctx.step_dev(t["u"].data_ptr(), t["v"].data_ptr(), t["w"].data_ptr(), t["theta"].data_ptr(),
                      [x.data_ptr() for x in d], [x.data_ptr() for x in big], p.data_ptr(),
                      [x.data_ptr() for x in dp])
@@ -293,12 +316,28 @@ def run_ours(args, rank, local, world):
                  d=[shp(pin(nf), fs) for _ in range(8)], big=[shp(pin(nb), bs) for _ in range(4)],
                  p=shp(pin(nf), fs), dp=[shp(pin(nd), ds) for _ in range(3)])
         ke = max(2, min(5, args.steps))
-        ctx.step(H["u"], H["v"], H["w"], H["th"], H["d"], H["big"], H["p"], H["dp"])   # warm-up
+
+        def host_step():
+            if not slab_mode:
+                ctx.step(H["u"], H["v"], H["w"], H["th"], H["d"], H["big"], H["p"], H["dp"])
+                return
+            # the slab step has no host variant: pinned host -> device, step, device -> host
+            t = S[0]
+            for k, hk in (("u", u), ("v", v), ("w", w), ("theta", th)):
+                t[k].copy_(torch.from_numpy(hk), non_blocking=True)
+            step(ctx, S)
+            outs = [(S[2][i], H["d"][i]) for i in range(8)] + [(S[3][i], H["big"][i]) for i in range(4)]
+            outs += [(S[4], H["p"])] + [(S[5][i], H["dp"][i]) for i in range(3)]
+            outs += [(t["u"], H["u"]), (t["v"], H["v"]), (t["w"], H["w"])]
+            for dsrc, hdst in outs:
+                torch.from_numpy(hdst.reshape(-1, order="F")).copy_(dsrc, non_blocking=True)
+            torch.cuda.synchronize()
+        host_step()   # warm-up
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(ke):
-            ctx.step(H["u"], H["v"], H["w"], H["th"], H["d"], H["big"], H["p"], H["dp"])
+            host_step()
         torch.cuda.synchronize()
         sec = (time.perf_counter() - t0) / ke
         if world > 1:
@@ -326,7 +365,9 @@ def run_ours(args, rank, local, world):
                    "precision": args.prec, "top_bc": "neumann",
                    "fp64_columns": ctx.info["n_fp64_columns"],
                    "l2": "inputs larger than L2 (one field = %.0f MB)" % (ctx.info["field_elems"] * es / 1e6),
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": (f"z-slabs x{world}: one {nx}x{ny}x{L * world}-level domain, "
+                                   "partitioned pressure solve, 2 all-gathers per step") if slab_mode
+                                  else f"replicas x{world}"},
         "step_roofline": {"bound": "hbm", "bytes_per_step": step_bytes, "achieved": round(step_gbs, 1),
                           "peak": hbm, "unit": "GB/s", "frac": round(step_gbs / hbm, 4),
                           "peak_kind": peak_kind},
@@ -398,6 +439,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--fp64-k2-max", type=float, default=-1.0,
                     help="mixed mode: k^2 bound of the FP64 TDMA columns (-1 = library default)")
+    ap.add_argument("--mode", choices=["slab", "replicas"], default="slab",
+                    help="N > 1: one z-split domain (slab) or independent instances (replicas)")
     ap.add_argument("--param", action="append", default=[],
                     help="execution tuning name=value passed to obl_set_param (e.g. fused=0)")
     args = ap.parse_args()

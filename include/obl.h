@@ -291,6 +291,31 @@ int obl_ensemble_time_dev(obl_ensemble *ens, const obl_step_io *ios, int use_gra
 int obl_ensemble_phase_times(obl_ensemble *ens, int on, double *ms, int n);
 int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n);
 
+/* ---- the step on a z-slab of a domain split over nranks ranks (one GPU each) ----
+   The reference splits z over npz MPI ranks and pipelines its Thomas sweeps rank by rank
+   with a send/recv per y-row (109_press_stag_array.f90:244-319, 103_flosol.f90:169-173).
+   Here each rank's context holds its slab (nzt = the rank's levels + 1, lz_tot its height:
+   level 0 and nz are the planes shared with the ranks below and above) and the solve is
+   partitioned: every rank eliminates its own rows, the ranks exchange two kinds of small
+   data through the caller's collectives, and every rank finishes its rows:
+     1. obl_slab_begin_dev: the forward pass of obl_step (ddx, ddy, zero_padding, RHS
+        spectra), the divtz planes (divtz_bot used on rank 0, divtz_top on rank nranks-1),
+        and plane_out = this rank's H_z(1) spectrum (plane_bytes);
+     2. caller: all-gather the planes; plane_above = the plane of rank+1 (ignored on the
+        top rank);
+     3. obl_slab_solve_dev: the rank's rows eliminated in FP64; iface_out = its interface
+        coefficients (iface_bytes, FP64);
+     4. caller: all-gather the interface coefficients, rank-major (nranks * iface_bytes);
+     5. obl_slab_finish_dev: the reduced 2*nranks-unknown system (redundantly), the rank's
+        p_hat and spectral dpdz, inverse transforms and project() with the rank's role
+        (jz_min = 2 and w(1) = 0 on rank 0; w(nz) = 0 and the stress-free copy on the top).
+   Levels 1..nz-1 of the outputs equal the single-domain obl_step at the same global
+   levels.  Only OBL_TOP_NEUMANN (npz >= 2 semantics); nranks <= 16. */
+int obl_slab_sizes(obl_ctx *ctx, long long *plane_bytes, long long *iface_bytes);
+int obl_slab_begin_dev(obl_ctx *ctx, const obl_step_io *io, int rank, int nranks, void *plane_out);
+int obl_slab_solve_dev(obl_ctx *ctx, const void *plane_above, int rank, int nranks, void *iface_out);
+int obl_slab_finish_dev(obl_ctx *ctx, const obl_step_io *io, const void *iface_all, int rank, int nranks);
+
 #ifdef __cplusplus
 }
 #endif

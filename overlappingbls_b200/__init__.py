@@ -49,6 +49,7 @@ EXPORTS = [
     "obl_ensemble_set_mode", "obl_ensemble_get_mode", "obl_ensemble_step_dev",
     "obl_ensemble_capture_dev", "obl_ensemble_replay", "obl_ensemble_synchronize",
     "obl_ensemble_time_dev", "obl_ensemble_phase_times", "obl_ensemble_last_error",
+    "obl_slab_sizes", "obl_slab_begin_dev", "obl_slab_solve_dev", "obl_slab_finish_dev",
 ]
 ENS_MODES = {"sequential": 0, "concurrent": 1, "persistent": 2, "persistent_split": 3}
 
@@ -146,6 +147,10 @@ def load_library(path=LIB_PATH):
         "obl_ensemble_synchronize": [E],
         "obl_ensemble_time_dev": [E, ctypes.POINTER(StepIO), I, I, I, DP],
         "obl_ensemble_phase_times": [E, I, DP, I],
+        "obl_slab_sizes": [ctx, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
+        "obl_slab_begin_dev": [ctx, ctypes.POINTER(StepIO), I, I, P],
+        "obl_slab_solve_dev": [ctx, P, I, I, P],
+        "obl_slab_finish_dev": [ctx, ctypes.POINTER(StepIO), P, I, I],
         "obl_ensemble_last_error": [E, ctypes.c_char_p, ctypes.c_size_t],
     })
     for name, args in sig.items():
@@ -393,6 +398,24 @@ class Context:
             io.dp[i] = dp[i]
         io.divtz_bot, io.divtz_top = divtz_bot, divtz_top
         self._check(self._lib.obl_step_dev(self._h, ctypes.byref(io)), "step_dev")
+
+    # ---- z-slab of a split domain (device pointers; see overlappingbls_b200/slab.py) ----
+    def slab_sizes(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self._lib.obl_slab_sizes(self._h, ctypes.byref(a), ctypes.byref(b)), "obl_slab_sizes")
+        return a.value, b.value
+
+    def slab_begin_dev(self, io, rank, nranks, plane_out):
+        self._check(self._lib.obl_slab_begin_dev(self._h, ctypes.byref(io), int(rank), int(nranks), plane_out),
+                    "obl_slab_begin_dev")
+
+    def slab_solve_dev(self, plane_above, rank, nranks, iface_out):
+        self._check(self._lib.obl_slab_solve_dev(self._h, plane_above, int(rank), int(nranks), iface_out),
+                    "obl_slab_solve_dev")
+
+    def slab_finish_dev(self, io, iface_all, rank, nranks):
+        self._check(self._lib.obl_slab_finish_dev(self._h, ctypes.byref(io), iface_all, int(rank), int(nranks)),
+                    "obl_slab_finish_dev")
 
     # ---- rollout problem of the adjoint (host arrays, float64) ----
     def convec(self, cx, cy, cz, u, v, w):

@@ -17,6 +17,7 @@
 #include "fused.cuh"
 #include "convec.cuh"
 #include "ensemble.cuh"
+#include "slab.cuh"
 
 using namespace obl;
 
@@ -61,6 +62,8 @@ struct obl_ctx {
     DevBuf rw_big[15];
     DevBuf ckpt;
     DevBuf ke;
+    // z-slab solve: FP64 particular solution, spikes, modified upper band
+    DevBuf slab_y, slab_v, slab_w, slab_cp;
     // tuning parameters (obl_set_param)
     long long param_fused = 0;          // use the cluster-fused kernels in obl_step
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
@@ -708,6 +711,112 @@ template <typename T> struct Ops {
         return OBL_OK;
     }
 
+    // ---- z-slab of a domain split over P ranks (slab.cuh) ----
+    // This context holds the rank's slab: levels 0..L of the rank (L = its interior levels),
+    // level 0 and L+1 being the planes it shares with the ranks below and above.
+    SlabArgs<T> slab_args(int rank, int P)
+    {
+        SlabArgs<T> a{};
+        a.Hx = (const C2<T> *)ctx->spec[0].p; a.Hy = (const C2<T> *)ctx->spec[1].p; a.Hz = (const C2<T> *)ctx->spec[2].p;
+        a.phat = (C2<T> *)ctx->spec[3].p; a.dph = (C2<T> *)ctx->spec[4].p;
+        a.y = (double2 *)ctx->slab_y.p; a.v = (double *)ctx->slab_v.p; a.w = (double *)ctx->slab_w.p;
+        a.cp = (double *)ctx->slab_cp.p;
+        a.kx = ctx->d_kx; a.ky = ctx->d_ky2;
+        a.S = ctx->sp(); a.lhx = ctx->lhx; a.nyt = ctx->nyt; a.L = ctx->L; a.dz = ctx->dz;
+        a.rank = rank; a.nranks = P;
+        return a;
+    }
+    // the rank's forward pass (ddx, ddy, zero_padding of u,v,w,theta and the RHS spectra),
+    // its boundary planes, and a copy of its H_z(1) plane for the rank below
+    int slab_begin(const obl_step_io *io, int rank, int P, C2<T> *plane_out)
+    {
+        const long long S = ctx->sp();
+        const size_t L = ctx->L, n = (size_t)S * L;
+        int rc;
+        if ((rc = ensure(ctx, ctx->slab_y, sizeof(double2) * n)) || (rc = ensure(ctx, ctx->slab_v, sizeof(double) * n)) ||
+            (rc = ensure(ctx, ctx->slab_w, sizeof(double) * n)) || (rc = ensure(ctx, ctx->slab_cp, sizeof(double) * n)))
+            return rc;
+        if ((rc = fwd_lines(io))) return rc;
+        C2<T> *Hz = (C2<T> *)ctx->spec[2].p;
+        const int ldx = ctx->ldx, ny = ctx->nyt, nx = ctx->nxt, lhx = ctx->lhx;
+        const double cst = 1.0 / ((double)nx * ny);
+        // H_z(0) of the bottom rank: divtz(:,:,1) (109_press_stag_array.f90:186-196)
+        if (rank == 0 && io->divtz_bot) {
+            auto ra = rowargs(io->divtz_bot, ldx, Hz, lhx, ny, cst, OP_FWD, nx);
+            if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
+        } else {
+            CK(cudaMemsetAsync(Hz, 0, sizeof(C2<T>) * S, s()));
+        }
+        // H_z(L+1) of the top rank: divtz(:,:,nz) (:197-200); the other ranks receive it
+        if (rank == P - 1 && io->divtz_top) {
+            auto ra = rowargs(io->divtz_top, ldx, Hz + S * (L + 1), lhx, ny, cst, OP_FWD, nx);
+            if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
+        } else {
+            CK(cudaMemsetAsync(Hz + S * (L + 1), 0, sizeof(C2<T>) * S, s()));
+        }
+        for (long long zb : {0LL, (long long)L + 1}) {
+            auto ca = colargs(Hz + S * zb, lhx, S, Hz + S * zb, lhx, S, lhx, 1, 1.0, OP_FWD, ny);
+            ca.zero_nyq = 1;
+            if ((rc = cols(OP_FWD, false, ny, ca, "press_bnd_cols"))) return rc;
+        }
+        CK(cudaMemcpyAsync(plane_out, Hz + S, sizeof(C2<T>) * S, cudaMemcpyDeviceToDevice, s()));
+        return OBL_OK;
+    }
+    int slab_solve(const C2<T> *plane_above, int rank, int P, double *iface_out)
+    {
+        const long long S = ctx->sp();
+        if (rank < P - 1)
+            CK(cudaMemcpyAsync((C2<T> *)ctx->spec[2].p + S * (ctx->L + 1), plane_above, sizeof(C2<T>) * S,
+                               cudaMemcpyDeviceToDevice, s()));
+        SlabArgs<T> a = slab_args(rank, P);
+        a.iface = iface_out;
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "slab_solve", s());
+        launch_slab_solve<T>(a, s(), e);
+        return chk(e, "slab_solve");
+    }
+    int slab_finish(const obl_step_io *io, const double *iface_all, int rank, int P)
+    {
+        const long long S = ctx->sp();
+        const int L = ctx->L, nx = ctx->nxt, ny = ctx->nyt, lhx = ctx->lhx, ldx = ctx->ldx;
+        int rc;
+        SlabArgs<T> a = slab_args(rank, P);
+        a.iface_all = iface_all;
+        {
+            cudaError_t e = cudaSuccess;
+            LaunchScope ls(ctx->rec, "slab_finish", s());
+            launch_slab_finish<T>(a, s(), e);
+            if ((rc = chk(e, "slab_finish"))) return rc;
+        }
+        C2<T> *Hx = (C2<T> *)ctx->spec[0].p, *Hy = (C2<T> *)ctx->spec[1].p, *Hz = (C2<T> *)ctx->spec[2].p;
+        C2<T> *ph = (C2<T> *)ctx->spec[3].p, *dph = (C2<T> *)ctx->spec[4].p;
+        PinvColArgs<T> pc{};
+        pc.ph = ph; pc.dph = dph; pc.Xp = Hz; pc.Xdx = Hx; pc.Xdy = Hy; pc.Xdz = dph;
+        pc.S = S; pc.lhx = lhx; pc.kx = ctx->d_kx; pc.ky = ctx->d_ky2; pc.twB = twt<T>(ctx, ny, ROLE_BWD);
+        {
+            LaunchScope ls(ctx->rec, "pinv_cols", s());
+            if ((rc = chk(PinvLaunch<T>::cols(ny, pc, L + 1, s()), "pinv_cols"))) return rc;
+        }
+        PinvRowArgs<T> pr{};
+        pr.Xp = Hz; pr.Xdx = Hx; pr.Xdy = Hy; pr.Xdz = dph;
+        pr.p = (T *)io->p; pr.dpdx = (T *)io->dp[0]; pr.dpdy = (T *)io->dp[1]; pr.dpdz = (T *)io->dp[2];
+        pr.u = (T *)io->u; pr.v = (T *)io->v; pr.w = (T *)io->w;
+        pr.npairs = (long long)ny * (L + 1) / 2;
+        pr.ldx = ldx; pr.ny = ny; pr.lhx = lhx;
+        pr.dt_tadv1 = (T)(ctx->dt_nd * kTadv1);
+        pr.twB = twt<T>(ctx, nx, ROLE_BWD);
+        pr.w_from_1 = rank > 0;   // jz_min = 2 only on the bottom rank (110_project.f90:29-33)
+        {
+            LaunchScope ls(ctx->rec, "pinv_rows_project", s());
+            if ((rc = chk(PinvLaunch<T>::rows(nx, pr, s()), "pinv_rows_project"))) return rc;
+        }
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "project_bc", s());
+        launch_project_bc_roles<T>((T *)io->u, (T *)io->v, (T *)io->w, ldx, ny, ctx->nz, (int)ctx->opt.ubc_stress_free,
+                                   rank == 0, rank == P - 1, s(), e);
+        return chk(e, "project_bc");
+    }
+
     // ---- ensemble: the arguments of this instance's units in the persistent kernel ----
     // The same arguments fwd_lines and press(rhs_ready, proj) give the line kernels, except
     // that the four x-padded intermediates (xpad4) are separate: all four fields' row units
@@ -1039,6 +1148,10 @@ int obl_ctx_destroy(obl_ctx *ctx)
     for (auto &b : ctx->rw_big) cudaFree(b.p);
     cudaFree(ctx->ckpt.p);
     cudaFree(ctx->ke.p);
+    cudaFree(ctx->slab_y.p);
+    cudaFree(ctx->slab_v.p);
+    cudaFree(ctx->slab_w.p);
+    cudaFree(ctx->slab_cp.p);
     for (auto &b : ctx->stage) cudaFree(b.p);
     for (auto &b : ctx->stage64) cudaFree(b.p);
     delete ctx;
@@ -1981,6 +2094,51 @@ int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n)
     std::strncpy(buf, ens->err.c_str(), n - 1);
     buf[n - 1] = 0;
     return OBL_OK;
+}
+
+} // extern "C"
+
+// ============================================================================= z-slab step
+static int slab_check(obl_ctx *ctx, int rank, int nranks)
+{
+    if (nranks < 1 || nranks > kSlabMaxRanks || rank < 0 || rank >= nranks)
+        return fail(ctx, OBL_ERR_ARG, "slab: need 0 <= rank < nranks <= " + std::to_string(kSlabMaxRanks));
+    if (ctx->opt.top_bc != OBL_TOP_NEUMANN)
+        return fail(ctx, OBL_ERR_UNSUPPORTED, "slab: a split domain has the npz >= 2 top (OBL_TOP_NEUMANN)");
+    if (ctx->L < 2) return fail(ctx, OBL_ERR_UNSUPPORTED, "slab: needs at least 2 levels per rank");
+    return OBL_OK;
+}
+
+extern "C" {
+
+int obl_slab_sizes(obl_ctx *ctx, long long *plane_bytes, long long *iface_bytes)
+{
+    if (!ctx) return OBL_ERR_ARG;
+    if (plane_bytes) *plane_bytes = (long long)(ctx->f64 ? sizeof(double2) : sizeof(float2)) * ctx->sp();
+    if (iface_bytes) *iface_bytes = (long long)sizeof(double) * kSlabIface * ctx->sp();
+    return OBL_OK;
+}
+
+int obl_slab_begin_dev(obl_ctx *ctx, const obl_step_io *io, int rank, int nranks, void *plane_out)
+{
+    if (!ctx || !step_io_ok(io) || !plane_out) return OBL_ERR_ARG;
+    if (int rc = slab_check(ctx, rank, nranks)) return rc;
+    DEVCALL(ctx, return o.slab_begin(io, rank, nranks, (C2<T> *)plane_out););
+}
+
+int obl_slab_solve_dev(obl_ctx *ctx, const void *plane_above, int rank, int nranks, void *iface_out)
+{
+    if (!ctx || !iface_out) return OBL_ERR_ARG;
+    if (int rc = slab_check(ctx, rank, nranks)) return rc;
+    if (rank < nranks - 1 && !plane_above) return fail(ctx, OBL_ERR_ARG, "slab: the plane of the rank above is missing");
+    DEVCALL(ctx, return o.slab_solve((const C2<T> *)plane_above, rank, nranks, (double *)iface_out););
+}
+
+int obl_slab_finish_dev(obl_ctx *ctx, const obl_step_io *io, const void *iface_all, int rank, int nranks)
+{
+    if (!ctx || !step_io_ok(io) || !iface_all) return OBL_ERR_ARG;
+    if (int rc = slab_check(ctx, rank, nranks)) return rc;
+    DEVCALL(ctx, return o.slab_finish(io, (const double *)iface_all, rank, nranks););
 }
 
 } // extern "C"

@@ -430,6 +430,8 @@ template <typename T> struct PinvRowArgs {
     int ldx, ny, lhx;
     T dt_tadv1;                           // dt*tadv1
     const C2<T> *twB;
+    int w_from_1;                         // 0: w updated from level 2 (bottom rank, jz_min = 2);
+                                          // 1: from level 1 (the z-slab of a rank above it)
 };
 
 // Unit u: warp w takes work item u*8 + w (twB in shared memory, scr = 8*LPW lines).
@@ -464,7 +466,7 @@ __device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long lon
         const C *X = q == 0 ? a.Xp : q == 1 ? a.Xdx : q == 2 ? a.Xdy : a.Xdz;
         T *out = q == 0 ? a.p + pl * z + off : (q == 1 ? a.dpdx : q == 2 ? a.dpdy : a.dpdz) + pl * (z - 1) + off;
         T *f = (q == 1 ? a.u : q == 2 ? a.v : a.w) + pl * z + off;
-        const bool proj = q == 1 || q == 2 || (q == 3 && z >= 2);   // jz_min = 2 for w
+        const bool proj = q == 1 || q == 2 || (q == 3 && z >= (a.w_from_1 ? 1 : 2));   // jz_min for w
         // the two rows of the field to update are read before the transform
         T fa[GL::PER * RL], fb[GL::PER * RL];
 #pragma unroll

@@ -1,0 +1,49 @@
+// slab.cuh -- the pressure solve of one z-slab of a domain split over P ranks.
+//
+// The reference splits z over npz ranks and pipelines the Thomas sweeps rank after rank
+// with send/recv per y-row (109_press_stag_array.f90:244-319).  Here every rank solves its
+// own rows of each (kx,ky) column at once (partitioned Thomas):
+//   solve:   T_loc y = r,  T_loc v = a_s e_1,  T_loc w = c_e e_m, where T_loc is the rank's
+//            block of the column's tridiagonal matrix without the two couplings a_s (to
+//            the last unknown of the rank below) and c_e (to the first of the rank above),
+//            so that x = y - v x_below - w x_above; the end values of y, v, w are the
+//            rank's interface coefficients (y_1, y_m complex; v_1, v_m, w_1, w_m real);
+//   (all ranks exchange their interface coefficients)
+//   finish:  the 2P interface unknowns (first and last of every rank) solve a 2x2-block
+//            tridiagonal system, redundantly on every rank; then x = y - v x_below -
+//            w x_above on the rank's rows, p_hat(0) and the spectral dpdz.
+// The block systems are diagonally dominant, so the split needs no pivoting.  The whole
+// solve runs in FP64 (the interface values are FP64 in every precision mode).
+#pragma once
+#include "fft.cuh"
+
+namespace obl {
+
+constexpr int kSlabMaxRanks = 16;
+constexpr int kSlabIface = 8;   // y1.re, y1.im, ym.re, ym.im, v1, vm, w1, wm per column
+
+template <typename T> struct SlabArgs {
+    const C2<T> *Hx, *Hy, *Hz;  // local spectra: Hx, Hy levels 1..L, Hz levels 0..L+1
+                                // (Hz(L+1): the first plane of the rank above, or the top plane)
+    C2<T> *phat, *dph;          // out (finish): p_hat levels 0..L, spectral dpdz levels 1..L
+    double2 *y;                 // scratch (S, L): particular solution
+    double *v, *w, *cp;         // scratch (S, L): spikes and the modified upper band
+    double *iface;              // out (solve): (S, kSlabIface)
+    const double *iface_all;    // in (finish): (P, S, kSlabIface)
+    const double *kx, *ky;      // kx(lhx), ky_2d row (nyt), Nyquist entries 0
+    long long S;
+    int lhx, nyt, L;
+    double dz;
+    int rank, nranks;
+};
+
+template <typename T> void launch_slab_solve(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e);
+template <typename T> void launch_slab_finish(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e);
+
+// project()'s boundary rows by rank role: bottom rank w(1) = 0, top rank w(nz) = 0 and
+// the stress-free copy (110_project.f90:50-60)
+template <typename T>
+void launch_project_bc_roles(T *u, T *v, T *w, int ldx, int nyt, int nz, int stress_free, int bottom, int top,
+                             cudaStream_t s, cudaError_t &e);
+
+} // namespace obl
