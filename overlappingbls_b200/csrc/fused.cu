@@ -142,14 +142,15 @@ template <typename T, int N> static cudaError_t pinv_cols_n(const PinvColArgs<T>
     using D = LineDerived<N, OP_INV>;
     const size_t sm = sizeof(C2<T>) * ((size_t)D::TB + (size_t)N * LmGeo<T>::WB);
     static bool init = false;
-    auto kern = k_cols_pinv<T, N>;
+    constexpr int NW = col_warps<T, N, OP_INV>();
+    auto kern = k_cols_pinv<T, N, NW>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         init = true;
     }
     dim3 grid((a.lhx + LmGeo<T>::WB - 1) / LmGeo<T>::WB, nlev);
-    kern<<<grid, 256, sm, s>>>(a);
+    kern<<<grid, 32 * NW, sm, s>>>(a);
     return cudaGetLastError();
 }
 

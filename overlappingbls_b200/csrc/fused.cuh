@@ -337,13 +337,13 @@ template <typename T> struct PinvColArgs {
 };
 
 // One CTA unit: line group bx of level z (twB in shared memory, buf = N*WB scratch).
-template <typename T, int N>
+template <typename T, int N, int NW = 8>
 __device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, int z, const C2<T> *twB, C2<T> *buf)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_INV>;
-    using G = LmGeo<T>;
-    constexpr int WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP_INV>::VR;
+    using G = LmGeo<T, NW>;
+    constexpr int WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP_INV, NW>::VR;
     constexpr int R0 = D::RB0, RL = D::RBL;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int line = lane % WB, t = lane / WB + (32 / WB) * warp;
@@ -406,8 +406,8 @@ __device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, 
     store(a.Xdz, w);
 }
 
-template <typename T, int N>
-__global__ void __launch_bounds__(256, 2) k_cols_pinv(PinvColArgs<T> a)
+template <typename T, int N, int NW>
+__global__ void __launch_bounds__(32 * NW, 2) k_cols_pinv(PinvColArgs<T> a)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_INV>;
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(256, 2) k_cols_pinv(PinvColArgs<T> a)
     C *buf = twB + D::TB;
     for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
     __syncthreads();
-    pinv_cols_unit<T, N>(a, blockIdx.x, blockIdx.y, twB, buf);
+    pinv_cols_unit<T, N, NW>(a, blockIdx.x, blockIdx.y, twB, buf);
 }
 
 // x-inverse of the four y-inverses and the projection (110_project.f90:16-40) in one

@@ -507,15 +507,23 @@ __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
 //   * the exchange scratch is line-minor (element i of line l at buf[i*WB + l]): a warp
 //     always touches consecutive words, so no pass has bank conflicts;
 //   * passes are separated by __syncthreads() because a line spans all warps.
-template <typename T> struct LmGeo {
+template <typename T, int NW_ = 8> struct LmGeo {
     static constexpr int WB = sizeof(T) == 4 ? 8 : 4;   // lines per CTA (64-byte row segments)
-    static constexpr int NW = 8;                          // warps per CTA
+    static constexpr int NW = NW_;                        // warps per CTA
     static constexpr int LL = (32 / WB) * NW;             // butterfly slots per line
 };
+// Warps per CTA of the standalone column kernels.  FP32 lines of 256 and more get 16
+// (twice the butterfly slots per line: half the registers per lane and twice the warps per
+// SM at the same shared memory), except the y-pad, which measured fastest with 8; FP64
+// (4 lines per CTA, already 64 slots per line) and the persistent ensemble units use 8.
+template <typename T, int N, int OP> constexpr int col_warps()
+{
+    return (sizeof(T) == 4 && N >= 256 && OP != OP_PAD) ? 16 : 8;
+}
 
-template <typename T, int N, int OP> struct ColDerived {
+template <typename T, int N, int OP, int NW = 8> struct ColDerived {
     using D = LineDerived<N, OP>;
-    static constexpr int LL = LmGeo<T>::LL;
+    static constexpr int LL = LmGeo<T, NW>::LL;
     static constexpr int rf = Regs<D::NI, LL, typename D::PF>::v, rb = Regs<D::NO, LL, typename D::PB>::v;
     static constexpr int VR = rf > rb ? rf : rb;
 };
@@ -523,15 +531,15 @@ template <typename T, int N, int OP> struct ColDerived {
 // One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
 // tables twF/twB are already in shared memory; buf is the exchange scratch (NM*WB).
 // Called by k_cols2 (one unit per CTA) and by the persistent ensemble kernel.
-template <typename T, int N, int OP, bool REAL>
+template <typename T, int N, int OP, bool REAL, int NW = 8>
 __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, const C2<T> *twF,
                                            const C2<T> *twB, C2<T> *buf)
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
     using D = LineDerived<N, OP>;
-    using G = LmGeo<T>;
-    constexpr int NI = D::NI, NO = D::NO, WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP>::VR;
+    using G = LmGeo<T, NW>;
+    constexpr int NI = D::NI, NO = D::NO, WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP, NW>::VR;
     (void)NI;
     (void)twF;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -646,8 +654,8 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
     }
 }
 
-template <typename T, int N, int OP, bool REAL>
-__global__ void __launch_bounds__(256) k_cols2(ColArgs<T> a)
+template <typename T, int N, int OP, bool REAL, int NW>
+__global__ void __launch_bounds__(32 * NW) k_cols2(ColArgs<T> a)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP>;
@@ -657,7 +665,7 @@ __global__ void __launch_bounds__(256) k_cols2(ColArgs<T> a)
     C *buf = twB + D::TB;
     load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
     __syncthreads();
-    cols2_unit<T, N, OP, REAL>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
+    cols2_unit<T, N, OP, REAL, NW>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
 }
 
 // ----------------------------------------------------------------------------- launchers
@@ -707,7 +715,8 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
 {
     static bool init = false;
     const size_t sm = cols2_smem<T, N, OP>();
-    auto kern = k_cols2<T, N, OP, REAL>;
+    constexpr int NW = col_warps<T, N, OP>();
+    auto kern = k_cols2<T, N, OP, REAL, NW>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
@@ -717,7 +726,7 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
     dim3 grid((nlines + WB - 1) / WB, a.nlev);
     if (grid.x < 1 || grid.y < 1) return cudaSuccess;
-    kern<<<grid, 256, sm, s>>>(a);
+    kern<<<grid, 32 * NW, sm, s>>>(a);
     return cudaGetLastError();
 }
 
