@@ -20,7 +20,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libobl_b200.so")
+# $OBL_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("OBL_LIB") or os.path.join(_HERE, "libobl_b200.so")
 
 OBL_OK = 0
 ERRORS = {1: "OBL_ERR_ARG", 2: "OBL_ERR_CUDA", 3: "OBL_ERR_NOMEM", 4: "OBL_ERR_TIMEOUT",

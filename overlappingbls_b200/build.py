@@ -1,9 +1,11 @@
 """Build libobl_b200.so (sm_100a) in-tree with nvcc.
 
-    python -m overlappingbls_b200.build [--force] [-j N]
+    python -m overlappingbls_b200.build [--force] [-j N] [-D NAME=VALUE ...] [--out PATH]
 
 Objects go to overlappingbls_b200/_build/ (git-ignored); the shared library is
-written next to this file so that it travels with the source tree.
+written next to this file so that it travels with the source tree.  -D passes
+compile-time tuning definitions (e.g. OBL_SIDX_SHIFT=4) and --out writes a variant
+library elsewhere (with its own object directory), loadable through $OBL_LIB.
 """
 import argparse
 import concurrent.futures as cf
@@ -33,49 +35,55 @@ def _deps():
     return max((os.path.getmtime(h) for h in hdrs), default=0.0)
 
 
-def _compile(src, force, hdr_mtime):
-    obj = os.path.join(BUILD, os.path.basename(src).replace(".cu", ".o"))
+def _compile(src, force, hdr_mtime, build_dir=BUILD, defines=()):
+    obj = os.path.join(build_dir, os.path.basename(src).replace(".cu", ".o"))
     if (not force and os.path.exists(obj)
             and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_mtime)):
         return obj, None
-    cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + ["-D" + d for d in defines] + FILE_FLAGS.get(os.path.basename(src), []) + \
+        ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, "$ " + " ".join(cmd) + "\n" + r.stdout + r.stderr
     return obj, None
 
 
-def build(force=False, jobs=None, verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(force=False, jobs=None, verbose=False, defines=(), out=None):
+    lib = out or LIB
+    build_dir = BUILD if out is None else os.path.join(os.path.dirname(os.path.abspath(out)), "_objs_" +
+                                                       os.path.basename(out).replace(".so", ""))
+    os.makedirs(build_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdr = _deps()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     objs, errs = [], []
     with cf.ThreadPoolExecutor(jobs) as ex:
-        for obj, err in ex.map(lambda s: _compile(s, force, hdr), srcs):
+        for obj, err in ex.map(lambda s: _compile(s, force, hdr, build_dir, defines), srcs):
             objs.append(obj)
             if err:
                 errs.append(err)
     if errs:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
     newest = max(os.path.getmtime(o) for o in objs)
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
+    if force or not os.path.exists(lib) or os.path.getmtime(lib) < newest:
+        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", lib] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     if verbose:
-        print(LIB)
-    return LIB
+        print(lib)
+    return lib
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-j", type=int, default=None)
+    ap.add_argument("-D", dest="defines", action="append", default=[])
+    ap.add_argument("--out", default=None)
     a = ap.parse_args()
     try:
-        build(force=a.force, jobs=a.j, verbose=True)
+        build(force=a.force, jobs=a.j, verbose=True, defines=a.defines, out=a.out)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

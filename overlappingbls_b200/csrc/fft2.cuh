@@ -95,8 +95,14 @@ template <int N, int NS, int R0, int... Rs> struct TwSize<N, NS, RPlan<R0, Rs...
 template <int N, class P> constexpr int tw_size() { return TwSize<N, 1, P>::v; }
 
 // scratch line length (complex) with one pad slot per 8 elements
-__host__ __device__ constexpr int scratch_len(int n) { return n + n / 8 + 1; }
-__device__ __forceinline__ int sidx(int i) { return i + (i >> 3); }
+// Per-line scratch with one pad element every 2^OBL_SIDX_SHIFT elements (a build-time
+// tuning knob; the column tiles below keep room for the default shift of 3 or more).
+#ifndef OBL_SIDX_SHIFT
+#define OBL_SIDX_SHIFT 5
+#endif
+static_assert(OBL_SIDX_SHIFT >= 3, "tile_rows assumes at most one pad element per 8");
+__host__ __device__ constexpr int scratch_len(int n) { return n + (n >> OBL_SIDX_SHIFT) + 1; }
+__device__ __forceinline__ int sidx(int i) { return i + (i >> OBL_SIDX_SHIFT); }
 
 // Scratch accessors: a padded contiguous line, a complex column of a shared tile, or
 // two adjacent real columns of a shared tile read as one complex line.  Tile rows are

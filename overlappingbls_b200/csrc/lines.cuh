@@ -507,8 +507,8 @@ __global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
 //   * the exchange scratch is line-minor (element i of line l at buf[i*WB + l]): a warp
 //     always touches consecutive words, so no pass has bank conflicts;
 //   * passes are separated by __syncthreads() because a line spans all warps.
-template <typename T, int NW_ = 8> struct LmGeo {
-    static constexpr int WB = sizeof(T) == 4 ? 8 : 4;   // lines per CTA (64-byte row segments)
+template <typename T, int NW_ = 8, int WB_ = (sizeof(T) == 4 ? 8 : 4)> struct LmGeo {
+    static constexpr int WB = WB_;                        // lines per CTA (WB*8-byte row segments)
     static constexpr int NW = NW_;                        // warps per CTA
     static constexpr int LL = (32 / WB) * NW;             // butterfly slots per line
 };
@@ -516,14 +516,25 @@ template <typename T, int NW_ = 8> struct LmGeo {
 // (twice the butterfly slots per line: half the registers per lane and twice the warps per
 // SM at the same shared memory), except the y-pad, which measured fastest with 8; FP64
 // (4 lines per CTA, already 64 slots per line) and the persistent ensemble units use 8.
+#ifndef OBL_PAD_NW
+#define OBL_PAD_NW 8
+#endif
+#ifndef OBL_PAD_WB
+#define OBL_PAD_WB 8
+#endif
 template <typename T, int N, int OP> constexpr int col_warps()
 {
-    return (sizeof(T) == 4 && N >= 256 && OP != OP_PAD) ? 16 : 8;
+    return (sizeof(T) == 4 && N >= 256) ? (OP == OP_PAD ? OBL_PAD_NW : 16) : 8;
+}
+// lines per CTA of the standalone column kernels (build-time knob for the FP32 y-pad)
+template <typename T, int N, int OP> constexpr int col_lines()
+{
+    return (sizeof(T) == 4 && N >= 256 && OP == OP_PAD) ? OBL_PAD_WB : LmGeo<T>::WB;
 }
 
-template <typename T, int N, int OP, int NW = 8> struct ColDerived {
+template <typename T, int N, int OP, int NW = 8, int WB = LmGeo<T>::WB> struct ColDerived {
     using D = LineDerived<N, OP>;
-    static constexpr int LL = LmGeo<T, NW>::LL;
+    static constexpr int LL = LmGeo<T, NW, WB>::LL;
     static constexpr int rf = Regs<D::NI, LL, typename D::PF>::v, rb = Regs<D::NO, LL, typename D::PB>::v;
     static constexpr int VR = rf > rb ? rf : rb;
 };
@@ -531,15 +542,15 @@ template <typename T, int N, int OP, int NW = 8> struct ColDerived {
 // One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
 // tables twF/twB are already in shared memory; buf is the exchange scratch (NM*WB).
 // Called by k_cols2 (one unit per CTA) and by the persistent ensemble kernel.
-template <typename T, int N, int OP, bool REAL, int NW = 8>
+template <typename T, int N, int OP, bool REAL, int NW = 8, int WB_ = LmGeo<T>::WB>
 __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, const C2<T> *twF,
                                            const C2<T> *twB, C2<T> *buf)
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
     using D = LineDerived<N, OP>;
-    using G = LmGeo<T, NW>;
-    constexpr int NI = D::NI, NO = D::NO, WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP, NW>::VR;
+    using G = LmGeo<T, NW, WB_>;
+    constexpr int NI = D::NI, NO = D::NO, WB = G::WB, LL = G::LL, VR = ColDerived<T, N, OP, NW, WB_>::VR;
     (void)NI;
     (void)twF;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -654,7 +665,7 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
     }
 }
 
-template <typename T, int N, int OP, bool REAL, int NW>
+template <typename T, int N, int OP, bool REAL, int NW, int WB>
 __global__ void __launch_bounds__(32 * NW) k_cols2(ColArgs<T> a)
 {
     using C = C2<T>;
@@ -665,7 +676,7 @@ __global__ void __launch_bounds__(32 * NW) k_cols2(ColArgs<T> a)
     C *buf = twB + D::TB;
     load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
     __syncthreads();
-    cols2_unit<T, N, OP, REAL, NW>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
+    cols2_unit<T, N, OP, REAL, NW, WB>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
 }
 
 // ----------------------------------------------------------------------------- launchers
@@ -705,24 +716,23 @@ template <typename T, int N, int OP> cudaError_t launch_rows_t(const RowArgs<T> 
     return cudaGetLastError();
 }
 
-template <typename T, int N, int OP> inline size_t cols2_smem()
+template <typename T, int N, int OP, int WB = LmGeo<T>::WB> inline size_t cols2_smem()
 {
     using D = LineDerived<N, OP>;
-    return sizeof(C2<T>) * ((size_t)D::TF + D::TB + (size_t)D::NM * LmGeo<T>::WB);
+    return sizeof(C2<T>) * ((size_t)D::TF + D::TB + (size_t)D::NM * WB);
 }
 
 template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const ColArgs<T> &a, cudaStream_t s)
 {
     static bool init = false;
-    const size_t sm = cols2_smem<T, N, OP>();
-    constexpr int NW = col_warps<T, N, OP>();
-    auto kern = k_cols2<T, N, OP, REAL, NW>;
+    constexpr int NW = col_warps<T, N, OP>(), WB = col_lines<T, N, OP>();
+    const size_t sm = cols2_smem<T, N, OP, WB>();
+    auto kern = k_cols2<T, N, OP, REAL, NW, WB>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         init = true;
     }
-    constexpr int WB = LmGeo<T>::WB;
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
     dim3 grid((nlines + WB - 1) / WB, a.nlev);
     if (grid.x < 1 || grid.y < 1) return cudaSuccess;

@@ -26,9 +26,13 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
 // Mixed precision in one launch: the first nbi blocks solve the FP64 island columns (their
 // long sequential FP64 sweeps start first), the remaining blocks the FP32 bulk columns,
 // so the two overlap instead of running back to back.  The sweeps are latency-bound: 8
-// blocks per SM (64 registers, a few FP64 spills) measured faster than 5 without spills.
+// blocks per SM (64 registers, a few FP64 spills) measured faster than 5 without spills
+// (OBL_TDMA_MINB is the build-time knob).
+#ifndef OBL_TDMA_MINB
+#define OBL_TDMA_MINB 8
+#endif
 template <typename T>
-__global__ void __launch_bounds__(128, 8) k_tdma_mixed(TdmaArgs<T> a, IslandArgs isl, int nbi)
+__global__ void __launch_bounds__(128, OBL_TDMA_MINB) k_tdma_mixed(TdmaArgs<T> a, IslandArgs isl, int nbi)
 {
     if ((int)blockIdx.x < nbi)
         tdma_column<T, double, true>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);

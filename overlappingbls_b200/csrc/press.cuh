@@ -28,6 +28,12 @@ struct IslandArgs {
     double2 *dscr;     // (n, L+1)
 };
 
+// levels the solve's loads run ahead of its recurrence
+#ifndef OBL_TDMA_AHEAD
+#define OBL_TDMA_AHEAD 4
+#endif
+constexpr int kTdmaAhead = OBL_TDMA_AHEAD;
+
 // One column's solve; t = the thread's index among the bulk columns or in the island list.
 template <typename TS, typename TC, bool ISLAND>
 __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandArgs &isl, long long t)
@@ -83,65 +89,97 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
     };
 
     // ---- forward elimination ----
-    // The RHS inputs of level iz+1 are loaded while level iz is eliminated (the loads are
-    // independent of the recurrence; issuing them ahead hides their latency).
+    // The sweep is latency-bound: every column of the problem is in flight at once, so the
+    // time per level is the load latency divided by how far ahead the loads run.  The RHS
+    // inputs of the next kTdmaAhead levels are kept in a ring of registers (storage type):
+    // slot s holds level base+s, refilled with level base+s+kTdmaAhead as soon as it is used.
+    constexpr int PF = kTdmaAhead;
+    using CS2 = C2<TS>;
+    auto raw = [&](const CS *p, int z) -> CS2 { return p[q + S * z]; };
+    auto cv = [&](CS2 v) -> CC { return mk<TC>((TC)v.x, (TC)v.y); };
     const CC hz0 = ld(a.Hz, 0);     // RHS_col(0) = H_z(0) (:209)
-    CC hzc = ld(a.Hz, 1);
-    CC hzn = ld(a.Hz, 2);
-    CC hx = ld(a.Hx, 1), hy = ld(a.Hy, 1);
+    CS2 rx[PF], ry[PF], rz[PF];
+#pragma unroll
+    for (int s = 0; s < PF; ++s) {
+        const int z = 1 + s;
+        rx[s] = raw(a.Hx, z <= L ? z : L);
+        ry[s] = raw(a.Hy, z <= L ? z : L);
+        rz[s] = raw(a.Hz, z <= L + 1 ? z : L + 1);
+    }
     CC dprev = hz0;
     TC cprev = 0;                   // coef_cp(0) = 0 on the bottom rank
-    for (int iz = 1; iz <= L; ++iz) {
-        const int izn = iz < L ? iz + 1 : iz;
-        const CC hx_n = ld(a.Hx, izn), hy_n = ld(a.Hy, izn), hz_n = ld(a.Hz, izn + 1);
-        TC am, bm, cm;
-        CC r;
-        if (!m00) {
-            const bool top = a.neumann_top && iz == L;
-            am = (iz == 1) ? (TC)0 : idz2;
-            bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (TC)2 * idz2);
-            cm = top ? (TC)0 : idz2;
-            const CC sxy = mk<TC>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
-            CC dh = csub(hzn, hzc);
-            if (iz == 1) dh = cadd(dh, hz0);
-            r = mk<TC>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
-        } else {
-            am = (iz == 1) ? (TC)0 : -idz;
-            bm = idz;
-            cm = 0;
-            r = (iz == 1) ? mk<TC>(0, 0) : hzc;
+    for (int base = 1; base <= L; base += PF) {
+#pragma unroll
+        for (int s = 0; s < PF; ++s) {
+            const int iz = base + s;
+            if (iz > L) break;
+            const CC hx = cv(rx[s]), hy = cv(ry[s]), hzc = cv(rz[s]);
+            const CC hzn = cv(rz[(s + 1) % PF]);   // level iz+1 (slot 0 was refilled at s = 0)
+            {
+                const int zn = iz + PF;
+                rx[s] = raw(a.Hx, zn <= L ? zn : L);
+                ry[s] = raw(a.Hy, zn <= L ? zn : L);
+                rz[s] = raw(a.Hz, zn <= L + 1 ? zn : L + 1);
+            }
+            TC am, bm, cm;
+            CC r;
+            if (!m00) {
+                const bool top = a.neumann_top && iz == L;
+                am = (iz == 1) ? (TC)0 : idz2;
+                bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (TC)2 * idz2);
+                cm = top ? (TC)0 : idz2;
+                const CC sxy = mk<TC>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
+                CC dh = csub(hzn, hzc);
+                if (iz == 1) dh = cadd(dh, hz0);
+                r = mk<TC>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+            } else {
+                am = (iz == 1) ? (TC)0 : -idz;
+                bm = idz;
+                cm = 0;
+                r = (iz == 1) ? mk<TC>(0, 0) : hzc;
+            }
+            const TC bp = bm - am * cprev;
+            const TC ibp = (TC)1 / bp;
+            const TC cp = cm * ibp;
+            const CC d = mk<TC>((r.x - am * dprev.x) * ibp, (r.y - am * dprev.y) * ibp);
+            st_c(iz, cp);
+            st_d(iz, d);
+            cprev = cp;
+            dprev = d;
         }
-        const TC bp = bm - am * cprev;
-        const TC ibp = (TC)1 / bp;
-        const TC cp = cm * ibp;
-        const CC d = mk<TC>((r.x - am * dprev.x) * ibp, (r.y - am * dprev.y) * ibp);
-        st_c(iz, cp);
-        st_d(iz, d);
-        cprev = cp;
-        dprev = d;
-        hzc = hzn;
-        hzn = hz_n;
-        hx = hx_n;
-        hy = hy_n;
     }
     // ---- back substitution ----
+    // the same ring for d(iz), c'(iz), iz = L-1 down to 1; the rows read ahead are below
+    // the ones already overwritten with p_hat, so the read-ahead never sees a p value
     CC pn = a.neumann_top ? dprev : mk<TC>(0, 0);   // p_hat(nz-1): solved row / forced 0
     ph[S * L] = mk<TS>((TS)pn.x, (TS)pn.y);
     C2<TS> *dph = a.dph ? a.dph + q : nullptr;
     const TC rdz = (TC)(1.0 / a.dz);
-    CC dn = L > 1 ? ld_d(L - 1) : mk<TC>(0, 0);
-    TC cn = L > 1 ? ld_c(L - 1) : (TC)0;
-    for (int iz = L - 1; iz >= 1; --iz) {
-        const CC d = dn;
-        const TC cp = cn;
-        if (iz > 1) {   // next level's operands ahead of this level's stores
-            dn = ld_d(iz - 1);
-            cn = ld_c(iz - 1);
+    CC rd[PF];
+    TC rc[PF];
+#pragma unroll
+    for (int s = 0; s < PF; ++s) {
+        const int z = L - 1 - s;
+        rd[s] = z >= 1 ? ld_d(z) : mk<TC>(0, 0);
+        rc[s] = z >= 1 ? ld_c(z) : (TC)0;
+    }
+    for (int base = L - 1; base >= 1; base -= PF) {
+#pragma unroll
+        for (int s = 0; s < PF; ++s) {
+            const int iz = base - s;
+            if (iz < 1) break;
+            const CC d = rd[s];
+            const TC cp = rc[s];
+            const int zn = iz - PF;
+            if (zn >= 1) {
+                rd[s] = ld_d(zn);
+                rc[s] = ld_c(zn);
+            }
+            const CC p = mk<TC>(d.x - cp * pn.x, d.y - cp * pn.y);
+            if (dph) dph[S * (iz + 1)] = mk<TS>((TS)((pn.x - p.x) * rdz), (TS)((pn.y - p.y) * rdz));
+            ph[S * iz] = mk<TS>((TS)p.x, (TS)p.y);
+            pn = p;
         }
-        const CC p = mk<TC>(d.x - cp * pn.x, d.y - cp * pn.y);
-        if (dph) dph[S * (iz + 1)] = mk<TS>((TS)((pn.x - p.x) * rdz), (TS)((pn.y - p.y) * rdz));
-        ph[S * iz] = mk<TS>((TS)p.x, (TS)p.y);
-        pn = p;
     }
     // Neumann ghost level below the wall (:313-315)
     const CC p0 = mk<TC>(pn.x - dz * hz0.x, pn.y - dz * hz0.y);
