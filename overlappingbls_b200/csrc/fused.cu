@@ -140,10 +140,13 @@ template struct RowsFwd3Launch<double>;
 template <typename T, int N> static cudaError_t pinv_cols_n(const PinvColArgs<T> &a, int nlev, cudaStream_t s)
 {
     using D = LineDerived<N, OP_INV>;
-    const size_t sm = sizeof(C2<T>) * ((size_t)D::TB + (size_t)N * LmGeo<T>::WB);
+    // (the 4-CTA shape of the other column kernels measured slower here: the four inverse
+    // transforms of one load need more than its 64 registers)
+    constexpr bool TWG = false;
+    constexpr int NW = TWG ? 8 : col_warps<T, N, OP_INV>();
+    const size_t sm = sizeof(C2<T>) * ((TWG ? 0 : (size_t)D::TB) + (size_t)N * LmGeo<T>::WB);
     static bool init = false;
-    constexpr int NW = col_warps<T, N, OP_INV>();
-    auto kern = k_cols_pinv<T, N, NW>;
+    auto kern = k_cols_pinv<T, N, NW, TWG>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;

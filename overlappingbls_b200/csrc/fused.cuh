@@ -406,17 +406,21 @@ __device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, 
     store(a.Xdz, w);
 }
 
-template <typename T, int N, int NW>
-__global__ void __launch_bounds__(32 * NW, 2) k_cols_pinv(PinvColArgs<T> a)
+template <typename T, int N, int NW, bool TWG = false>
+__global__ void __launch_bounds__(32 * NW, TWG ? 4 : 2) k_cols_pinv(PinvColArgs<T> a)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_INV>;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C *twB = reinterpret_cast<C *>(smraw);
-    C *buf = twB + D::TB;
-    for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
-    __syncthreads();
-    pinv_cols_unit<T, N, NW>(a, blockIdx.x, blockIdx.y, twB, buf);
+    if constexpr (TWG) {   // twiddles through L1 (see col_tw_global)
+        pinv_cols_unit<T, N, NW>(a, blockIdx.x, blockIdx.y, a.twB, reinterpret_cast<C *>(smraw));
+    } else {
+        C *twB = reinterpret_cast<C *>(smraw);
+        C *buf = twB + D::TB;
+        for (int i = threadIdx.x; i < D::TB; i += blockDim.x) twB[i] = a.twB[i];
+        __syncthreads();
+        pinv_cols_unit<T, N, NW>(a, blockIdx.x, blockIdx.y, twB, buf);
+    }
 }
 
 // x-inverse of the four y-inverses and the projection (110_project.f90:16-40) in one

@@ -516,6 +516,12 @@ template <typename T, int NW_ = 8, int WB_ = (sizeof(T) == 4 ? 8 : 4)> struct Lm
 // (twice the butterfly slots per line: half the registers per lane and twice the warps per
 // SM at the same shared memory), except the y-pad, which measured fastest with 8; FP64
 // (4 lines per CTA, already 64 slots per line) and the persistent ensemble units use 8.
+#ifndef OBL_PAD_TWG
+#define OBL_PAD_TWG 1
+#endif
+#ifndef OBL_COLS_TWG
+#define OBL_COLS_TWG 1
+#endif
 #ifndef OBL_PAD_NW
 #define OBL_PAD_NW 8
 #endif
@@ -524,7 +530,20 @@ template <typename T, int NW_ = 8, int WB_ = (sizeof(T) == 4 ? 8 : 4)> struct Lm
 #endif
 template <typename T, int N, int OP> constexpr int col_warps()
 {
-    return (sizeof(T) == 4 && N >= 256) ? (OP == OP_PAD ? OBL_PAD_NW : 16) : 8;
+    return (sizeof(T) == 4 && N >= 256) ? (OP == OP_PAD ? OBL_PAD_NW
+                                                        : ((OBL_COLS_TWG && (OP == OP_DERIV || OP == OP_FWD)) ? 8 : 16))
+                                        : 8;
+}
+// Twiddles read through L1 instead of staged in shared memory, with the registers bounded
+// for 4 CTAs per SM (4 independent CTAs in different phases of their load / transform /
+// store cycle instead of 3, or 2 of 16 warps).  For the FP32 y-pad of long lines this
+// frees the 11.5 KB of tables that kept it at 3 CTAs per SM: 23% faster.  OBL_COLS_TWG
+// applies the same shape (8 warps) to ddy and the forward y-transform: 24% and 19% faster
+// than 16-warp CTAs with staged tables.
+template <typename T, int N, int OP> constexpr bool col_tw_global()
+{
+    return sizeof(T) == 4 && N >= 256 &&
+           ((OP == OP_PAD && OBL_PAD_TWG) || ((OP == OP_DERIV || OP == OP_FWD) && OBL_COLS_TWG));
 }
 // lines per CTA of the standalone column kernels (build-time knob for the FP32 y-pad)
 template <typename T, int N, int OP> constexpr int col_lines()
@@ -665,18 +684,22 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
     }
 }
 
-template <typename T, int N, int OP, bool REAL, int NW, int WB>
-__global__ void __launch_bounds__(32 * NW) k_cols2(ColArgs<T> a)
+template <typename T, int N, int OP, bool REAL, int NW, int WB, bool TWG = false>
+__global__ void __launch_bounds__(32 * NW, TWG ? 4 : 1) k_cols2(ColArgs<T> a)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP>;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C *twF = reinterpret_cast<C *>(smraw);
-    C *twB = twF + D::TF;
-    C *buf = twB + D::TB;
-    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
-    __syncthreads();
-    cols2_unit<T, N, OP, REAL, NW, WB>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
+    if constexpr (TWG) {
+        cols2_unit<T, N, OP, REAL, NW, WB>(a, blockIdx.x, blockIdx.y, a.twF, a.twB, reinterpret_cast<C *>(smraw));
+    } else {
+        C *twF = reinterpret_cast<C *>(smraw);
+        C *twB = twF + D::TF;
+        C *buf = twB + D::TB;
+        load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
+        __syncthreads();
+        cols2_unit<T, N, OP, REAL, NW, WB>(a, blockIdx.x, blockIdx.y, twF, twB, buf);
+    }
 }
 
 // ----------------------------------------------------------------------------- launchers
@@ -726,8 +749,10 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
 {
     static bool init = false;
     constexpr int NW = col_warps<T, N, OP>(), WB = col_lines<T, N, OP>();
-    const size_t sm = cols2_smem<T, N, OP, WB>();
-    auto kern = k_cols2<T, N, OP, REAL, NW, WB>;
+    constexpr bool TWG = col_tw_global<T, N, OP>();
+    using D = LineDerived<N, OP>;
+    const size_t sm = TWG ? sizeof(C2<T>) * (size_t)D::NM * WB : cols2_smem<T, N, OP, WB>();
+    auto kern = k_cols2<T, N, OP, REAL, NW, WB, TWG>;
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
