@@ -50,6 +50,7 @@ struct obl_ctx {
     int n_isl = 0;
     int *d_isl = nullptr;
     unsigned char *d_skip = nullptr;
+    int *d_isl_slot = nullptr;   // column -> island index, -1 for the bulk (z-slab solve)
     // work buffers
     DevBuf spec[5];            // Hx, Hy, Hz, phat, dpdz spectrum (lhx*nyt*(nz+1) complex)
     DevBuf cscr;               // c' scratch
@@ -62,8 +63,10 @@ struct obl_ctx {
     DevBuf rw_big[15];
     DevBuf ckpt;
     DevBuf ke;
-    // z-slab solve: FP64 particular solution, spikes, modified upper band
+    // z-slab solve: particular solution, spikes, modified upper band; bulk columns in the
+    // storage type, FP64 island columns of the mixed mode apart
     DevBuf slab_y, slab_v, slab_w, slab_cp;
+    DevBuf slab_iy, slab_iv, slab_iw, slab_icp;
     // tuning parameters (obl_set_param)
     long long param_fused = 0;          // use the cluster-fused kernels in obl_step
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
@@ -736,8 +739,13 @@ template <typename T> struct Ops {
         SlabArgs<T> a{};
         a.Hx = (const C2<T> *)ctx->spec[0].p; a.Hy = (const C2<T> *)ctx->spec[1].p; a.Hz = (const C2<T> *)ctx->spec[2].p;
         a.phat = (C2<T> *)ctx->spec[3].p; a.dph = (C2<T> *)ctx->spec[4].p;
-        a.y = (double2 *)ctx->slab_y.p; a.v = (double *)ctx->slab_v.p; a.w = (double *)ctx->slab_w.p;
-        a.cp = (double *)ctx->slab_cp.p;
+        a.y = (C2<T> *)ctx->slab_y.p; a.v = (T *)ctx->slab_v.p; a.w = (T *)ctx->slab_w.p;
+        a.cp = (T *)ctx->slab_cp.p;
+        a.n_isl = ctx->n_isl;
+        a.isl_cols = ctx->n_isl ? ctx->d_isl : nullptr;
+        a.isl_slot = ctx->n_isl ? ctx->d_isl_slot : nullptr;
+        a.iy = (double2 *)ctx->slab_iy.p; a.iv = (double *)ctx->slab_iv.p; a.iw = (double *)ctx->slab_iw.p;
+        a.icp = (double *)ctx->slab_icp.p;
         a.kx = ctx->d_kx; a.ky = ctx->d_ky2;
         a.S = ctx->sp(); a.lhx = ctx->lhx; a.nyt = ctx->nyt; a.L = ctx->L; a.dz = ctx->dz;
         a.rank = rank; a.nranks = P;
@@ -748,10 +756,12 @@ template <typename T> struct Ops {
     int slab_begin(const obl_step_io *io, int rank, int P, C2<T> *plane_out)
     {
         const long long S = ctx->sp();
-        const size_t L = ctx->L, n = (size_t)S * L;
+        const size_t L = ctx->L, n = (size_t)S * L, ni = (size_t)(ctx->n_isl > 0 ? ctx->n_isl : 1) * L;
         int rc;
-        if ((rc = ensure(ctx, ctx->slab_y, sizeof(double2) * n)) || (rc = ensure(ctx, ctx->slab_v, sizeof(double) * n)) ||
-            (rc = ensure(ctx, ctx->slab_w, sizeof(double) * n)) || (rc = ensure(ctx, ctx->slab_cp, sizeof(double) * n)))
+        if ((rc = ensure(ctx, ctx->slab_y, sizeof(C2<T>) * n)) || (rc = ensure(ctx, ctx->slab_v, sizeof(T) * n)) ||
+            (rc = ensure(ctx, ctx->slab_w, sizeof(T) * n)) || (rc = ensure(ctx, ctx->slab_cp, sizeof(T) * n)) ||
+            (rc = ensure(ctx, ctx->slab_iy, sizeof(double2) * ni)) || (rc = ensure(ctx, ctx->slab_iv, sizeof(double) * ni)) ||
+            (rc = ensure(ctx, ctx->slab_iw, sizeof(double) * ni)) || (rc = ensure(ctx, ctx->slab_icp, sizeof(double) * ni)))
             return rc;
         if ((rc = fwd_lines(io))) return rc;
         C2<T> *Hz = (C2<T> *)ctx->spec[2].p;
@@ -1133,10 +1143,14 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
             }
         ctx->n_isl = (int)cols.size();
         if (ctx->n_isl) {
+            std::vector<int> slot(skip.size(), -1);
+            for (size_t k = 0; k < cols.size(); ++k) slot[(size_t)cols[k]] = (int)k;
             if (cudaMalloc(&ctx->d_isl, sizeof(int) * cols.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
             if (cudaMalloc(&ctx->d_skip, skip.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            if (cudaMalloc(&ctx->d_isl_slot, sizeof(int) * slot.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
             cudaMemcpy(ctx->d_isl, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice);
             cudaMemcpy(ctx->d_skip, skip.data(), skip.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(ctx->d_isl_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice);
         }
     }
     *out = ctx;
@@ -1169,6 +1183,11 @@ int obl_ctx_destroy(obl_ctx *ctx)
     cudaFree(ctx->slab_v.p);
     cudaFree(ctx->slab_w.p);
     cudaFree(ctx->slab_cp.p);
+    cudaFree(ctx->slab_iy.p);
+    cudaFree(ctx->slab_iv.p);
+    cudaFree(ctx->slab_iw.p);
+    cudaFree(ctx->slab_icp.p);
+    cudaFree(ctx->d_isl_slot);
     for (auto &b : ctx->stage) cudaFree(b.p);
     for (auto &b : ctx->stage64) cudaFree(b.p);
     if (ctx->cin) cudaStreamDestroy(ctx->cin);

@@ -9,11 +9,20 @@
 
 namespace obl {
 
-template <typename T>
-__global__ void __launch_bounds__(128) k_slab_solve(SlabArgs<T> a)
+// The rank's rows of one column in precision TC; t = the column (bulk) or island index.
+template <typename T, typename TC, bool ISLAND>
+__device__ __forceinline__ void slab_column(const SlabArgs<T> &a, long long t)
 {
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= a.S) return;
+    using CC = C2<TC>;
+    long long q;
+    if constexpr (ISLAND) {
+        if (t >= a.n_isl) return;
+        q = a.isl_cols[t];
+    } else {
+        if (t >= a.S) return;
+        q = t;
+        if (a.isl_slot && a.isl_slot[q] >= 0) return;   // solved by an island thread
+    }
     const long long S = a.S;
     const int L = a.L;
     double *f = a.iface + q * kSlabIface;
@@ -22,74 +31,95 @@ __global__ void __launch_bounds__(128) k_slab_solve(SlabArgs<T> a)
         for (int k = 0; k < kSlabIface; ++k) f[k] = 0.0;
         return;
     }
-    const double kxd = a.kx[ix], kyd = a.ky[iy], k2 = kxd * kxd + kyd * kyd;
-    const bool m00 = k2 == 0.0;
+    const double kxd = a.kx[ix], kyd = a.ky[iy], k2d = kxd * kxd + kyd * kyd;
+    const bool m00 = k2d == 0.0;
     const bool bot = a.rank == 0, topr = a.rank == a.nranks - 1;
-    const double dz = a.dz, idz = 1.0 / dz, idz2 = 1.0 / (dz * dz);
-    auto ld = [&](const C2<T> *p, int z) -> double2 {
+    const TC kx = (TC)kxd, ky = (TC)kyd, k2 = (TC)k2d;
+    const TC dz = (TC)a.dz, idz = (TC)(1.0 / a.dz), idz2 = (TC)(1.0 / (a.dz * a.dz));
+    auto ld = [&](const C2<T> *p, int z) -> CC {
         const C2<T> v = p[q + S * z];
-        return make_double2((double)v.x, (double)v.y);
+        return mk<TC>((TC)v.x, (TC)v.y);
     };
-    const double2 hz0 = ld(a.Hz, 0);
-    double cprev = 0.0, vp = 0.0, wp = 0.0;
-    double2 yp = make_double2(0.0, 0.0);
+    auto o = [&](int j) -> long long { return ISLAND ? t + (long long)a.n_isl * (j - 1) : q + S * (j - 1); };
+    auto st = [&](int j, TC cpj, CC yj, TC vj, TC wj) {
+        const long long k = o(j);
+        if constexpr (ISLAND) {
+            a.icp[k] = cpj; a.iy[k] = make_double2(yj.x, yj.y); a.iv[k] = vj; a.iw[k] = wj;
+        } else {
+            a.cp[k] = (T)cpj; a.y[k] = mk<T>((T)yj.x, (T)yj.y); a.v[k] = (T)vj; a.w[k] = (T)wj;
+        }
+    };
+    auto ldy = [&](int j) -> CC {
+        if constexpr (ISLAND) { const double2 v = a.iy[o(j)]; return mk<TC>(v.x, v.y); }
+        else { const C2<T> v = a.y[o(j)]; return mk<TC>((TC)v.x, (TC)v.y); }
+    };
+    auto lds = [&](const T *b, const double *ib, int j) -> TC {
+        if constexpr (ISLAND) return ib[o(j)];
+        else return (TC)b[o(j)];
+    };
+    const CC hz0 = ld(a.Hz, 0);
+    TC cprev = 0, vp = 0, wp = 0;
+    CC yp = mk<TC>(0, 0);
     for (int j = 1; j <= L; ++j) {
         const bool b1 = bot && j == 1, tl = topr && j == L;
-        double am, bm, cm;
-        double2 r;
+        TC am, bm, cm;
+        CC r;
         if (!m00) {
-            am = b1 ? 0.0 : idz2;
-            cm = tl ? 0.0 : idz2;
-            bm = (b1 || tl) ? -(k2 + idz2) : -(k2 + 2.0 * idz2);
-            const double2 hx = ld(a.Hx, j), hy = ld(a.Hy, j), hzc = ld(a.Hz, j), hzn = ld(a.Hz, j + 1);
-            double dx = hzn.x - hzc.x, dy = hzn.y - hzc.y;
+            am = b1 ? (TC)0 : idz2;
+            cm = tl ? (TC)0 : idz2;
+            bm = (b1 || tl) ? -(k2 + idz2) : -(k2 + (TC)2 * idz2);
+            const CC hx = ld(a.Hx, j), hy = ld(a.Hy, j), hzc = ld(a.Hz, j), hzn = ld(a.Hz, j + 1);
+            TC dx = hzn.x - hzc.x, dy = hzn.y - hzc.y;
             if (b1) {
                 dx += hz0.x;
                 dy += hz0.y;
             }
-            const double sx = kxd * hx.x + kyd * hy.x, sy = kxd * hx.y + kyd * hy.y;
-            r = make_double2(-sy + dx / dz, sx + dy / dz);
+            const TC sx = kx * hx.x + ky * hy.x, sy = kx * hx.y + ky * hy.y;
+            r = mk<TC>(-sy + dx / dz, sx + dy / dz);
         } else {
-            am = b1 ? 0.0 : -idz;
+            am = b1 ? (TC)0 : -idz;
             bm = idz;
-            cm = 0.0;
-            r = b1 ? make_double2(0.0, 0.0) : ld(a.Hz, j);
+            cm = 0;
+            r = b1 ? mk<TC>(0, 0) : ld(a.Hz, j);
         }
-        const double asub = j == 1 ? 0.0 : am;   // a_1 couples to the rank below
-        const double csup = j == L ? 0.0 : cm;   // c_L couples to the rank above
-        const double iden = 1.0 / (bm - asub * cprev);
-        const double cpj = csup * iden;
-        yp = make_double2((r.x - asub * yp.x) * iden, (r.y - asub * yp.y) * iden);
-        vp = ((j == 1 ? am : 0.0) - asub * vp) * iden;
-        wp = ((j == L ? cm : 0.0) - asub * wp) * iden;
-        const long long o = q + S * (j - 1);
-        a.cp[o] = cpj;
-        a.y[o] = yp;
-        a.v[o] = vp;
-        a.w[o] = wp;
+        const TC asub = j == 1 ? (TC)0 : am;   // a_1 couples to the rank below
+        const TC csup = j == L ? (TC)0 : cm;   // c_L couples to the rank above
+        const TC iden = (TC)1 / (bm - asub * cprev);
+        const TC cpj = csup * iden;
+        yp = mk<TC>((r.x - asub * yp.x) * iden, (r.y - asub * yp.y) * iden);
+        vp = ((j == 1 ? am : (TC)0) - asub * vp) * iden;
+        wp = ((j == L ? cm : (TC)0) - asub * wp) * iden;
+        st(j, cpj, yp, vp, wp);
         cprev = cpj;
     }
-    double2 yn = yp;
-    double vn = vp, wn = wp;
+    CC yn = yp;
+    TC vn = vp, wn = wp;
     f[2] = yn.x;
     f[3] = yn.y;
     f[5] = vn;
     f[7] = wn;
     for (int j = L - 1; j >= 1; --j) {
-        const long long o = q + S * (j - 1);
-        const double c = a.cp[o];
-        const double2 yj = a.y[o];
-        yn = make_double2(yj.x - c * yn.x, yj.y - c * yn.y);
-        vn = a.v[o] - c * vn;
-        wn = a.w[o] - c * wn;
-        a.y[o] = yn;
-        a.v[o] = vn;
-        a.w[o] = wn;
+        const TC c = lds(a.cp, a.icp, j);
+        const CC yj = ldy(j);
+        yn = mk<TC>(yj.x - c * yn.x, yj.y - c * yn.y);
+        vn = lds(a.v, a.iv, j) - c * vn;
+        wn = lds(a.w, a.iw, j) - c * wn;
+        st(j, c, yn, vn, wn);
     }
     f[0] = yn.x;
     f[1] = yn.y;
     f[4] = vn;
     f[6] = wn;
+}
+
+// island blocks first (their FP64 sweeps are the longest), then the bulk columns
+template <typename T>
+__global__ void __launch_bounds__(128) k_slab_solve(SlabArgs<T> a, int nbi)
+{
+    if ((int)blockIdx.x < nbi)
+        slab_column<T, double, true>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    else
+        slab_column<T, T, false>(a, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
@@ -141,11 +171,23 @@ __global__ void __launch_bounds__(128) k_slab_finish(SlabArgs<T> a)
     // the rank's rows, p_hat(0) (the last unknown of the rank below, or the Neumann ghost
     // p_hat(1) - dz*H_z(0) on rank 0, 109_press_stag_array.f90:313-315) and dpdz
     const double dz = a.dz, rdz = 1.0 / dz;
+    const int slot = a.isl_slot ? a.isl_slot[q] : -1;
     double2 xprev = below;
     for (int j = 1; j <= L; ++j) {
-        const long long o = q + S * (j - 1);
-        const double2 yj = a.y[o];
-        const double vj = a.v[o], wj = a.w[o];
+        double2 yj;
+        double vj, wj;
+        if (slot >= 0) {
+            const long long o = slot + (long long)a.n_isl * (j - 1);
+            yj = a.iy[o];
+            vj = a.iv[o];
+            wj = a.iw[o];
+        } else {
+            const long long o = q + S * (j - 1);
+            const C2<T> yv = a.y[o];
+            yj = make_double2((double)yv.x, (double)yv.y);
+            vj = (double)a.v[o];
+            wj = (double)a.w[o];
+        }
         const double2 x = make_double2(yj.x - vj * below.x - wj * above.x, yj.y - vj * below.y - wj * above.y);
         if (j == 1 && r == 0) {
             const C2<T> h = a.Hz[q];
@@ -177,7 +219,8 @@ __global__ void k_project_bc_roles(T *u, T *v, T *w, int ldx, int nyt, int nz, i
 template <typename T> void launch_slab_solve(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_slab_solve<T><<<(unsigned)((a.S + 127) / 128), 128, 0, s>>>(a);
+    const int nbi = (a.n_isl + 127) / 128, nbb = (int)((a.S + 127) / 128);
+    k_slab_solve<T><<<(unsigned)(nbi + nbb), 128, 0, s>>>(a, nbi);
     e = cudaGetLastError();
 }
 template <typename T> void launch_slab_finish(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e)

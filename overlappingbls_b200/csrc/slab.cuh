@@ -12,8 +12,10 @@
 //   finish:  the 2P interface unknowns (first and last of every rank) solve a 2x2-block
 //            tridiagonal system, redundantly on every rank; then x = y - v x_below -
 //            w x_above on the rank's rows, p_hat(0) and the spectral dpdz.
-// The block systems are diagonally dominant, so the split needs no pivoting.  The whole
-// solve runs in FP64 (the interface values are FP64 in every precision mode).
+// The block systems are diagonally dominant, so the split needs no pivoting.  The rank's
+// elimination runs in the storage precision for the bulk columns and in FP64 for the
+// island columns of the mixed mode (as the single-domain solve does); the interface values
+// and the reduced system are FP64 in every mode.
 #pragma once
 #include "fft.cuh"
 
@@ -26,8 +28,13 @@ template <typename T> struct SlabArgs {
     const C2<T> *Hx, *Hy, *Hz;  // local spectra: Hx, Hy levels 1..L, Hz levels 0..L+1
                                 // (Hz(L+1): the first plane of the rank above, or the top plane)
     C2<T> *phat, *dph;          // out (finish): p_hat levels 0..L, spectral dpdz levels 1..L
-    double2 *y;                 // scratch (S, L): particular solution
-    double *v, *w, *cp;         // scratch (S, L): spikes and the modified upper band
+    C2<T> *y;                   // bulk scratch (S, L) in the storage type: particular solution,
+    T *v, *w, *cp;              // spikes and the modified upper band
+    const int *isl_cols;        // mixed mode: the FP64 columns (k^2 small), solved in FP64 with
+    const int *isl_slot;        // their own scratch (n_isl, L); isl_slot[q] = island index or -1
+    int n_isl;
+    double2 *iy;
+    double *iv, *iw, *icp;
     double *iface;              // out (solve): (S, kSlabIface)
     const double *iface_all;    // in (finish): (P, S, kSlabIface)
     const double *kx, *ky;      // kx(lhx), ky_2d row (nyt), Nyquist entries 0
