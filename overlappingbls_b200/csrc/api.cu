@@ -65,8 +65,8 @@ struct obl_ctx {
     DevBuf ke;
     // z-slab solve: particular solution, spikes, modified upper band; bulk columns in the
     // storage type, FP64 island columns of the mixed mode apart
-    DevBuf slab_y, slab_v, slab_w, slab_cp;
-    DevBuf slab_iy, slab_iv, slab_iw, slab_icp;
+    DevBuf slab_v, slab_cp;
+    DevBuf slab_iy, slab_iv, slab_icp;
     // tuning parameters (obl_set_param)
     long long param_fused = 0;          // use the cluster-fused kernels in obl_step
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
@@ -739,12 +739,12 @@ template <typename T> struct Ops {
         SlabArgs<T> a{};
         a.Hx = (const C2<T> *)ctx->spec[0].p; a.Hy = (const C2<T> *)ctx->spec[1].p; a.Hz = (const C2<T> *)ctx->spec[2].p;
         a.phat = (C2<T> *)ctx->spec[3].p; a.dph = (C2<T> *)ctx->spec[4].p;
-        a.y = (C2<T> *)ctx->slab_y.p; a.v = (T *)ctx->slab_v.p; a.w = (T *)ctx->slab_w.p;
+        a.v = (T *)ctx->slab_v.p;
         a.cp = (T *)ctx->slab_cp.p;
         a.n_isl = ctx->n_isl;
         a.isl_cols = ctx->n_isl ? ctx->d_isl : nullptr;
         a.isl_slot = ctx->n_isl ? ctx->d_isl_slot : nullptr;
-        a.iy = (double2 *)ctx->slab_iy.p; a.iv = (double *)ctx->slab_iv.p; a.iw = (double *)ctx->slab_iw.p;
+        a.iy = (double2 *)ctx->slab_iy.p; a.iv = (double *)ctx->slab_iv.p;
         a.icp = (double *)ctx->slab_icp.p;
         a.kx = ctx->d_kx; a.ky = ctx->d_ky2;
         a.S = ctx->sp(); a.lhx = ctx->lhx; a.nyt = ctx->nyt; a.L = ctx->L; a.dz = ctx->dz;
@@ -758,10 +758,9 @@ template <typename T> struct Ops {
         const long long S = ctx->sp();
         const size_t L = ctx->L, n = (size_t)S * L, ni = (size_t)(ctx->n_isl > 0 ? ctx->n_isl : 1) * L;
         int rc;
-        if ((rc = ensure(ctx, ctx->slab_y, sizeof(C2<T>) * n)) || (rc = ensure(ctx, ctx->slab_v, sizeof(T) * n)) ||
-            (rc = ensure(ctx, ctx->slab_w, sizeof(T) * n)) || (rc = ensure(ctx, ctx->slab_cp, sizeof(T) * n)) ||
+        if ((rc = ensure(ctx, ctx->slab_v, sizeof(T) * n)) || (rc = ensure(ctx, ctx->slab_cp, sizeof(T) * n)) ||
             (rc = ensure(ctx, ctx->slab_iy, sizeof(double2) * ni)) || (rc = ensure(ctx, ctx->slab_iv, sizeof(double) * ni)) ||
-            (rc = ensure(ctx, ctx->slab_iw, sizeof(double) * ni)) || (rc = ensure(ctx, ctx->slab_icp, sizeof(double) * ni)))
+            (rc = ensure(ctx, ctx->slab_icp, sizeof(double) * ni)))
             return rc;
         if ((rc = fwd_lines(io))) return rc;
         C2<T> *Hz = (C2<T> *)ctx->spec[2].p;
@@ -1179,13 +1178,10 @@ int obl_ctx_destroy(obl_ctx *ctx)
     for (auto &b : ctx->rw_big) cudaFree(b.p);
     cudaFree(ctx->ckpt.p);
     cudaFree(ctx->ke.p);
-    cudaFree(ctx->slab_y.p);
     cudaFree(ctx->slab_v.p);
-    cudaFree(ctx->slab_w.p);
     cudaFree(ctx->slab_cp.p);
     cudaFree(ctx->slab_iy.p);
     cudaFree(ctx->slab_iv.p);
-    cudaFree(ctx->slab_iw.p);
     cudaFree(ctx->slab_icp.p);
     cudaFree(ctx->d_isl_slot);
     for (auto &b : ctx->stage) cudaFree(b.p);

@@ -6,12 +6,15 @@
 //   solve:   T_loc y = r,  T_loc v = a_s e_1,  T_loc w = c_e e_m, where T_loc is the rank's
 //            block of the column's tridiagonal matrix without the two couplings a_s (to
 //            the last unknown of the rank below) and c_e (to the first of the rank above),
-//            so that x = y - v x_below - w x_above; the end values of y, v, w are the
-//            rank's interface coefficients (y_1, y_m complex; v_1, v_m, w_1, w_m real);
+//            so that x = y - v x_below - w x_above.  The forward elimination keeps the
+//            eliminated rows (c'_j, y'_j, v'_j; w' is zero above the last row); a back
+//            recurrence in registers gives the end values of y, v, w: the rank's interface
+//            coefficients (y_1, y_m complex; v_1, v_m, w_1, w_m real);
 //   (all ranks exchange their interface coefficients)
 //   finish:  the 2P interface unknowns (first and last of every rank) solve a 2x2-block
-//            tridiagonal system, redundantly on every rank; then x = y - v x_below -
-//            w x_above on the rank's rows, p_hat(0) and the spectral dpdz.
+//            tridiagonal system, redundantly on every rank; then the back substitution
+//            x_j = y'_j - v'_j x_below - c'_j x_{j+1} (x_{m+1} = x_above, the last row with
+//            w'_m) on the rank's rows, p_hat(0) and the spectral dpdz.
 // The block systems are diagonally dominant, so the split needs no pivoting.  The rank's
 // elimination runs in the storage precision for the bulk columns and in FP64 for the
 // island columns of the mixed mode (as the single-domain solve does); the interface values
@@ -27,14 +30,14 @@ constexpr int kSlabIface = 8;   // y1.re, y1.im, ym.re, ym.im, v1, vm, w1, wm pe
 template <typename T> struct SlabArgs {
     const C2<T> *Hx, *Hy, *Hz;  // local spectra: Hx, Hy levels 1..L, Hz levels 0..L+1
                                 // (Hz(L+1): the first plane of the rank above, or the top plane)
-    C2<T> *phat, *dph;          // out (finish): p_hat levels 0..L, spectral dpdz levels 1..L
-    C2<T> *y;                   // bulk scratch (S, L) in the storage type: particular solution,
-    T *v, *w, *cp;              // spikes and the modified upper band
+    C2<T> *phat, *dph;          // out (finish): p_hat levels 0..L, spectral dpdz levels 1..L;
+                                // between the kernels phat levels 1..L hold y'
+    T *v, *cp;                  // bulk scratch (S, L) in the storage type: v', c'
     const int *isl_cols;        // mixed mode: the FP64 columns (k^2 small), solved in FP64 with
     const int *isl_slot;        // their own scratch (n_isl, L); isl_slot[q] = island index or -1
     int n_isl;
     double2 *iy;
-    double *iv, *iw, *icp;
+    double *iv, *icp;
     double *iface;              // out (solve): (S, kSlabIface)
     const double *iface_all;    // in (finish): (P, S, kSlabIface)
     const double *kx, *ky;      // kx(lhx), ky_2d row (nyt), Nyquist entries 0
