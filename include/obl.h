@@ -119,6 +119,17 @@ int obl_ddz_w(obl_ctx *ctx, double *dfdz, const double *fun);
 int obl_ddz_uv_dev(obl_ctx *ctx, void *dfdz, const void *fun);
 int obl_ddz_w_dev(obl_ctx *ctx, void *dfdz, const void *fun);
 
+/* ---- stress divergence: divstress_uv / divstress_w (107_divstress.f90:4-44, 48-104) ----
+   tx, ty, tz, divt (ldx,nyt,0:nz); single-rank roles (the domain holds the wall and the
+   top).  divstress_uv: divt = ddx(tx) + ddy(ty) + ddz_w(tz) on levels 1..nz-1, BOGUS
+   on levels 0 and nz.  divstress_w: divt = ddx(tx) + ddy(ty) on level 1 and nz, plus
+   ddz_uv(tz) on levels 2..nz-1, BOGUS on level 0.  The x pads (nxt, nxt+1) of the
+   computed levels are 0.  divt must not alias an input. */
+int obl_divstress_uv(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz);
+int obl_divstress_w(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz);
+int obl_divstress_uv_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz);
+int obl_divstress_w_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz);
+
 /* ---- 2D transforms fftn_mpi / ifftn_mpi (203_fftn_mpi.f90:4-35, 39-67) ----
    in (ldx, nyt, nlev) real -> out (lhx, nyt, nlev) complex, unnormalised, x- and
    y-Nyquist zeroed; ifftn: complex -> real, x < nxt written. */

@@ -411,6 +411,54 @@ void orc_ddz_w(const orc_grid *g, double *dfdz, const double *fun)
 }
 
 /* ------------------------------------------------------------------------- */
+/* stress divergence (107_divstress.f90:4-104), single rank (coordz == 0 ==    */
+/* npz-1): the three derivative arrays in full, then the level-by-level sum     */
+/* ------------------------------------------------------------------------- */
+static void divstress(const orc_grid *g, double *divt, const double *tx, const double *ty,
+                      const double *tz, int w_form)
+{
+    int nxt = g->nxt, nyt = g->nyt, ldx = g->ldx, nz = g->nz;
+    size_t pl = (size_t)ldx * nyt, n = pl * (size_t)(nz + 1);
+    double *dx = (double *)calloc(n, sizeof(double));
+    double *dy = (double *)calloc(n, sizeof(double));
+    double *dz = (double *)calloc(n, sizeof(double));
+    orc_ddx(g, dx, tx, nz + 1);                    /* :21, :67 */
+    orc_ddy(g, dy, ty, nz + 1);                    /* :24, :71 */
+    if (w_form) orc_ddz_uv(g, dz, tz);             /* :76: levels 2..nz-1 */
+    else orc_ddz_w(g, dz, tz);                     /* :27: levels 0..nz-1 */
+    int top = w_form ? nz : nz - 1;
+    for (int z = 1; z <= top; z++)
+        for (int y = 0; y < nyt; y++) {
+            size_t r = (size_t)ldx * y + pl * z;
+            for (int x = 0; x < nxt; x++) {
+                double v = dx[r + x] + dy[r + x];
+                /* uv: :36-37; w: the wall level (coordz == 0, :85) and the top level
+                   (coordz == npz-1, :98) take no vertical term, :91-92 the rest */
+                if (!w_form || (z >= 2 && z <= nz - 1)) v += dz[r + x];
+                divt[r + x] = v;
+            }
+            divt[r + nxt] = 0.0;                   /* :40, :95, :99 */
+            divt[r + nxt + 1] = 0.0;
+        }
+    for (size_t q = 0; q < pl; q++) divt[q] = BOGUS;                 /* :41, :79 */
+    if (!w_form)
+        for (size_t q = 0; q < pl; q++) divt[q + pl * nz] = BOGUS;   /* :42 */
+    free(dx);
+    free(dy);
+    free(dz);
+}
+
+void orc_divstress_uv(const orc_grid *g, double *divt, const double *tx, const double *ty, const double *tz)
+{
+    divstress(g, divt, tx, ty, tz, 0);
+}
+
+void orc_divstress_w(const orc_grid *g, double *divt, const double *tx, const double *ty, const double *tz)
+{
+    divstress(g, divt, tx, ty, tz, 1);
+}
+
+/* ------------------------------------------------------------------------- */
 /* 2D transforms (203_fftn_mpi.f90:4-67), npy = 1                              */
 /* ------------------------------------------------------------------------- */
 void orc_fftn(const orc_grid *g, const double *in, cplx *out)

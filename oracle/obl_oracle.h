@@ -67,6 +67,10 @@ void orc_ddy(const orc_grid *g, double *dfdy, const double *fun, int nlev);
 void orc_ddz_uv(const orc_grid *g, double *dfdz, const double *fun);
 void orc_ddz_w(const orc_grid *g, double *dfdz, const double *fun);
 
+/* 107_divstress.f90:4-44 / 48-104, single rank: divt (ldx,nyt,0:nz) fully written */
+void orc_divstress_uv(const orc_grid *g, double *divt, const double *tx, const double *ty, const double *tz);
+void orc_divstress_w(const orc_grid *g, double *divt, const double *tx, const double *ty, const double *tz);
+
 /* ---- 2D transforms of one plane (203_fftn_mpi.f90:4-67) ---- */
 void orc_fftn(const orc_grid *g, const double *in, double complex *out);
 void orc_ifftn(const orc_grid *g, const double complex *in, double *out);

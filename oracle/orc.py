@@ -64,6 +64,8 @@ def lib():
             "orc_ddy": (None, [G, P, P, I]),
             "orc_ddz_uv": (None, [G, P, P]),
             "orc_ddz_w": (None, [G, P, P]),
+            "orc_divstress_uv": (None, [G, P, P, P, P]),
+            "orc_divstress_w": (None, [G, P, P, P, P]),
             "orc_fftn": (None, [G, P, P]),
             "orc_ifftn": (None, [G, P, P]),
             "orc_zero_padding": (None, [G, P, P]),
@@ -193,6 +195,16 @@ class Grid:
     def ddz_w(self, f, out=None):
         out = np.zeros_like(f, order="F") if out is None else out
         lib().orc_ddz_w(self.ref, _p(out), _p(f))
+        return out
+
+    def divstress_uv(self, tx, ty, tz):
+        out = np.zeros_like(tx, order="F")
+        lib().orc_divstress_uv(self.ref, _p(out), _p(tx), _p(ty), _p(tz))
+        return out
+
+    def divstress_w(self, tx, ty, tz):
+        out = np.zeros_like(tx, order="F")
+        lib().orc_divstress_w(self.ref, _p(out), _p(tx), _p(ty), _p(tz))
         return out
 
     def fftn(self, plane):

@@ -36,6 +36,7 @@ EXPORTS = [
     "obl_set_param", "obl_get_param",
     "obl_ddx", "obl_ddy", "obl_ddx_dev", "obl_ddy_dev",
     "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
+    "obl_divstress_uv", "obl_divstress_w", "obl_divstress_uv_dev", "obl_divstress_w_dev",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
     "obl_zero_padding", "obl_zero_unpadding", "obl_zero_padding_dev", "obl_zero_unpadding_dev",
     "obl_zero_padding_noalloc_dev",
@@ -116,6 +117,8 @@ def load_library(path=LIB_PATH):
         "obl_ddx_dev": [ctx, P, P, I], "obl_ddy_dev": [ctx, P, P, I],
         "obl_ddz_uv": [ctx, P, P], "obl_ddz_w": [ctx, P, P],
         "obl_ddz_uv_dev": [ctx, P, P], "obl_ddz_w_dev": [ctx, P, P],
+        "obl_divstress_uv": [ctx, P, P, P, P], "obl_divstress_w": [ctx, P, P, P, P],
+        "obl_divstress_uv_dev": [ctx, P, P, P, P], "obl_divstress_w_dev": [ctx, P, P, P, P],
         "obl_fftn": [ctx, P, P, I], "obl_ifftn": [ctx, P, P, I],
         "obl_fftn_dev": [ctx, P, P, I], "obl_ifftn_dev": [ctx, P, P, I],
         "obl_zero_padding": [ctx, P, P, I], "obl_zero_unpadding": [ctx, P, P, I],
@@ -299,6 +302,16 @@ class Context:
     def ddz_w(self, dfdz, fun):
         self._check(self._lib.obl_ddz_w(self._h, _ptr(dfdz), _ptr(fun)), "ddz_w")
 
+    def divstress_uv(self, divt, tx, ty, tz):
+        """divt = div of the stress row (tx, ty, tz) at uv nodes (107_divstress.f90:4-44)."""
+        self._check(self._lib.obl_divstress_uv(self._h, _ptr(divt), _ptr(tx), _ptr(ty), _ptr(tz)),
+                    "divstress_uv")
+
+    def divstress_w(self, divt, tx, ty, tz):
+        """divt = div of the stress row (tx, ty, tz) at w nodes (107_divstress.f90:48-104)."""
+        self._check(self._lib.obl_divstress_w(self._h, _ptr(divt), _ptr(tx), _ptr(ty), _ptr(tz)),
+                    "divstress_w")
+
     def fftn(self, fin, fout):
         self._check(self._lib.obl_fftn(self._h, _ptr(fin), _ptr(fout, np.complex128),
                                        self._nlev(fin)), "fftn")
@@ -356,6 +369,18 @@ class Context:
 
     def ddy_dev(self, dfdy, fun, nlev):
         self._check(self._lib.obl_ddy_dev(self._h, dfdy, fun, nlev), "ddy_dev")
+
+    def ddz_uv_dev(self, dfdz, fun):
+        self._check(self._lib.obl_ddz_uv_dev(self._h, dfdz, fun), "ddz_uv_dev")
+
+    def ddz_w_dev(self, dfdz, fun):
+        self._check(self._lib.obl_ddz_w_dev(self._h, dfdz, fun), "ddz_w_dev")
+
+    def divstress_uv_dev(self, divt, tx, ty, tz):
+        self._check(self._lib.obl_divstress_uv_dev(self._h, divt, tx, ty, tz), "divstress_uv_dev")
+
+    def divstress_w_dev(self, divt, tx, ty, tz):
+        self._check(self._lib.obl_divstress_w_dev(self._h, divt, tx, ty, tz), "divstress_w_dev")
 
     def zero_padding_dev(self, var, var_big, nlev):
         self._check(self._lib.obl_zero_padding_dev(self._h, var, var_big, nlev), "zero_padding_dev")

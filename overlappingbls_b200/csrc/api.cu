@@ -18,6 +18,7 @@
 #include "convec.cuh"
 #include "ensemble.cuh"
 #include "slab.cuh"
+#include "divstress.cuh"
 
 using namespace obl;
 
@@ -421,6 +422,42 @@ template <typename T> struct Ops {
         LaunchScope ls(ctx->rec, "ddz_w", s());
         launch_ddz_w<T>(d, f, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
         return chk(e, "ddz_w");
+    }
+
+    // ---- divstress_uv / divstress_w (107_divstress.f90:4-104), single-rank roles ----
+    // ddx(tx) into divt's computed levels, then the ddy(ty) column pass whose stores add
+    // it, the vertical difference of tz and the zero pads; BOGUS on the other levels.
+    int divstress(T *divt, const T *tx, const T *ty, const T *tz, bool w_form)
+    {
+        const int nz = ctx->nz, nlev = w_form ? nz : nz - 1;   // levels 1..nlev
+        const long long pl = ctx->plane();
+        auto ra = rowargs(tx + pl, ctx->ldx, divt + pl, ctx->ldx, (long long)ctx->nyt * nlev, 1.0 / ctx->nxt,
+                          OP_DERIV, ctx->nxt);
+        ra.ktab = ctx->d_kx;
+        int rc = rows(OP_DERIV, ctx->nxt, ra, "divt_ddx_rows");
+        if (rc) return rc;
+        auto ca = colargs(ty + pl, ctx->ldx, pl, divt + pl, ctx->ldx, pl, ctx->nxt, nlev, 1.0 / ctx->nyt, OP_DERIV,
+                          ctx->nyt);
+        ca.ktab = ctx->d_ky1;
+        DivEpi<T> ep{};
+        ep.out = divt + pl;
+        ep.tz = tz + pl;
+        ep.row = ctx->ldx;
+        ep.plane = pl;
+        ep.ncols = ctx->nxt;
+        ep.rdz = (T)(1.0 / ctx->dz);
+        ep.fwd = w_form ? 0 : 1;
+        ep.zlo = w_form ? 1 : 0;            // divstress_w: no dz(tzz) on the wall level (:81-85)
+        ep.zhi = w_form ? nz - 2 : nlev - 1; // ... nor on the top level (:97-98)
+        {
+            LaunchScope ls(ctx->rec, "divt_ddy_cols", s());
+            if ((rc = chk(launch_cols_divt<T>(ctx->nyt, ca, ep, s()), "divt_ddy_cols"))) return rc;
+        }
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "divt_bogus", s());
+        launch_fill<T>(divt, pl, (T)-1234567890.0, s(), e);   // BOGUS, 001_param.f90:40
+        if (!w_form) launch_fill<T>(divt + pl * nz, pl, (T)-1234567890.0, s(), e);
+        return chk(e, "divt_bogus");
     }
 
     // ---- the fused step ----
@@ -1340,6 +1377,16 @@ int obl_ddz_uv_dev(obl_ctx *ctx, void *dfdz, const void *fun)
     if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
     DEVCALL(ctx, return o.ddz_uv((T *)dfdz, (const T *)fun););
 }
+int obl_divstress_uv_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz)
+{
+    if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.divstress((T *)divt, (const T *)tx, (const T *)ty, (const T *)tz, false););
+}
+int obl_divstress_w_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz)
+{
+    if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2) return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.divstress((T *)divt, (const T *)tx, (const T *)ty, (const T *)tz, true););
+}
 int obl_ddz_w_dev(obl_ctx *ctx, void *dfdz, const void *fun)
 {
     if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
@@ -1443,6 +1490,24 @@ int obl_ddz_uv(obl_ctx *ctx, double *dfdz, const double *fun)
     // whole array back after staging the host output too, so untouched levels survive
     std::vector<HArg> a{harg_in(fun, n), harg_out(dfdz, n, true, ctx->ldx, ctx->ldx, 0, nyt * (ctx->nz + 1))};
     HOSTCALL(double, ctx, a, return o.ddz_uv((T *)d[1], (const T *)d[0]););
+}
+static int divstress_host(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz,
+                          bool w_form)
+{
+    if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2) return OBL_ERR_ARG;
+    const long long n = ctx->field(), nyt = ctx->nyt;
+    std::vector<HArg> a{harg_in(tx, n), harg_in(ty, n), harg_in(tz, n),
+                        harg_out(divt, n, false, ctx->ldx, ctx->ldx, 0, nyt * (ctx->nz + 1))};
+    HOSTCALL(double, ctx, a,
+             return o.divstress((T *)d[3], (const T *)d[0], (const T *)d[1], (const T *)d[2], w_form););
+}
+int obl_divstress_uv(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz)
+{
+    return divstress_host(ctx, divt, tx, ty, tz, false);
+}
+int obl_divstress_w(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz)
+{
+    return divstress_host(ctx, divt, tx, ty, tz, true);
 }
 int obl_ddz_w(obl_ctx *ctx, double *dfdz, const double *fun)
 {

@@ -558,12 +558,19 @@ template <typename T, int N, int OP, int NW = 8, int WB = LmGeo<T>::WB> struct C
     static constexpr int VR = rf > rb ? rf : rb;
 };
 
+// Store hook of the column kernel's backward output: epi(z, i, line, x) may change the
+// value x of row i, line `line` of plane z just before it is stored.  The default does
+// nothing and compiles away.
+struct NoColEpi {
+    template <class C> __device__ __forceinline__ void operator()(int, int, int, C &) const {}
+};
+
 // One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
 // tables twF/twB are already in shared memory; buf is the exchange scratch (NM*WB).
 // Called by k_cols2 (one unit per CTA) and by the persistent ensemble kernel.
-template <typename T, int N, int OP, bool REAL, int NW = 8, int WB_ = LmGeo<T>::WB>
+template <typename T, int N, int OP, bool REAL, int NW = 8, int WB_ = LmGeo<T>::WB, class EPI = NoColEpi>
 __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, const C2<T> *twF,
-                                           const C2<T> *twB, C2<T> *buf)
+                                           const C2<T> *twB, C2<T> *buf, const EPI &epi = EPI())
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
@@ -672,6 +679,7 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
                             x.x += cref.x;
                             x.y += cref.y;
                         }
+                        epi(z, i, gl, x);
                         gst(i, x);
                         if constexpr (OP == OP_UNPAD && REAL) {
                             // var(nxt+1:ldx,:) = var(1:2,:) (108_01_padd.f90:195)
