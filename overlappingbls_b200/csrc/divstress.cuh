@@ -39,6 +39,17 @@ template <typename T> struct DivEpi {
         if (line == 0)
             *reinterpret_cast<C2<T> *>(out + (long long)z * plane + (long long)i * row + ncols) = mk<T>(0, 0);
     }
+    // The loads above sit between stores to the same array, so they cannot be hoisted:
+    // without this each would wait for HBM at store time.
+    __device__ __forceinline__ void prefetch(int z, int i, int line) const
+    {
+        const long long o = (long long)z * plane + (long long)i * row + 2 * line;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(out + o));
+        if (z >= zlo && z <= zhi) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(tz + o + (fwd ? plane : 0)));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(tz + o - (fwd ? 0 : plane)));
+        }
+    }
 };
 
 // ddy of the real columns of a (ldx, nyt, nlev) field with the DivEpi store hook

@@ -559,10 +559,13 @@ template <typename T, int N, int OP, int NW = 8, int WB = LmGeo<T>::WB> struct C
 };
 
 // Store hook of the column kernel's backward output: epi(z, i, line, x) may change the
-// value x of row i, line `line` of plane z just before it is stored.  The default does
+// value x of row i, line `line` of plane z just before it is stored; epi.prefetch(z, i,
+// line) is called for the same elements when the line is loaded, before its transforms,
+// so that what the hook reads is on chip by the time it is stored.  The default does
 // nothing and compiles away.
 struct NoColEpi {
     template <class C> __device__ __forceinline__ void operator()(int, int, int, C &) const {}
+    __device__ __forceinline__ void prefetch(int, int, int) const {}
 };
 
 // One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
@@ -615,6 +618,18 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
                     x.y = (x.y - cref.y) * a.scale;
                 }
                 v[b * D::RF0 + r] = x;
+            }
+        }
+        if constexpr (!std::is_same<EPI, NoColEpi>::value) {
+            using GP = Geo<NO, D::RBL, LL>;
+            if (act) {
+#pragma unroll
+                for (int b = 0; b < GP::PER; ++b) {
+                    const int j = t + LL * b;
+                    if (GP::FULL || j < GP::NB)
+#pragma unroll
+                        for (int r = 0; r < D::RBL; ++r) epi.prefetch(z, j + r * GP::NB, gl);
+                }
             }
         }
         fft_regs<NI, typename D::PF, LL, true, true>(v, sc, twF, t);

@@ -18,6 +18,7 @@ use iso_c_binding
 implicit none
 private
 public :: obl_gpu_init, obl_gpu_finalize, ddx_gpu, ddy_gpu, ddz_uv_gpu, ddz_w_gpu, &
+          divstress_uv_gpu, divstress_w_gpu, &
           zero_padding_gpu, zero_unpadding_gpu, filter_data_gpu, fftn_gpu, ifftn_gpu, &
           press_stag_array_gpu, dpdz_gpu, project_gpu, obl_gpu_check
 
@@ -73,6 +74,18 @@ interface
         type(c_ptr), value :: c
         real(c_double), dimension(*) :: dfdz
         real(c_double), dimension(*), intent(in) :: fun
+    end function
+    integer(c_int) function obl_divstress_uv(c, divt, tx, ty, tz) bind(C, name="obl_divstress_uv")
+        import :: c_int, c_ptr, c_double
+        type(c_ptr), value :: c
+        real(c_double), dimension(*) :: divt
+        real(c_double), dimension(*), intent(in) :: tx, ty, tz
+    end function
+    integer(c_int) function obl_divstress_w(c, divt, tx, ty, tz) bind(C, name="obl_divstress_w")
+        import :: c_int, c_ptr, c_double
+        type(c_ptr), value :: c
+        real(c_double), dimension(*) :: divt
+        real(c_double), dimension(*), intent(in) :: tx, ty, tz
     end function
     integer(c_int) function obl_ddz_w(c, dfdz, fun) bind(C, name="obl_ddz_w")
         import :: c_int, c_ptr, c_double
@@ -194,6 +207,18 @@ subroutine ddz_uv_gpu(dfdz, fun)               ! 004_derivatives.f90:85-116
     real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(in) :: fun
     real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(inout) :: dfdz
     call obl_gpu_check(obl_ddz_uv(ctx, dfdz, fun), 'ddz_uv')
+end subroutine
+
+subroutine divstress_uv_gpu(divt, tx, ty, tz)   ! 107_divstress.f90:4-44
+    real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(in) :: tx, ty, tz
+    real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(out) :: divt
+    call obl_gpu_check(obl_divstress_uv(ctx, divt, tx, ty, tz), 'divstress_uv')
+end subroutine
+
+subroutine divstress_w_gpu(divt, tx, ty, tz)    ! 107_divstress.f90:48-104
+    real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(in) :: tx, ty, tz
+    real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(out) :: divt
+    call obl_gpu_check(obl_divstress_w(ctx, divt, tx, ty, tz), 'divstress_w')
 end subroutine
 
 subroutine ddz_w_gpu(dfdz, fun)                ! 004_derivatives.f90:155-183
