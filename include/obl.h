@@ -42,6 +42,7 @@ extern "C" {
 #define OBL_ERR_TIMEOUT 4     /* a bounded device-side wait expired            */
 #define OBL_ERR_UNSUPPORTED 5 /* grid size without a compiled FFT plan         */
 #define OBL_ERR_NODEV 6       /* no CUDA device                                */
+#define OBL_ERR_IO 7          /* file open, read or write failed; short file    */
 
 /* ---- precision modes ---- */
 #define OBL_PREC_F64 0   /* every kernel in FP64 (the plain FP64 GPU form)             */
@@ -129,6 +130,32 @@ int obl_divstress_uv(obl_ctx *ctx, double *divt, const double *tx, const double 
 int obl_divstress_w(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz);
 int obl_divstress_uv_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz);
 int obl_divstress_w_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz);
+
+/* ---- restart files: write_file_mpi_3d / read_file_mpi_3d (202_parallel.f90:1084-1120,
+   1211-1250), checkpoint_final (012_io.f90:496-546), read_flow_field
+   (102_01_ic.f90:682-734), total_time.dat (012_io.f90:485-490, 102_01_ic.f90:697-705) ----
+   A field in a file is the global FP64 array (nxt, nyt, nzranks*(nz-1)) in Fortran order
+   at byte offset disp0: levels 1..nz-1 of every z-rank, rank zrank's block at z offset
+   zrank*(nz-1) (MPI subarray start (0, 0, (nz-1)*coordz) with npy = 1).  var is a device
+   field (ldx,nyt,0:nz) in the storage type; FP32 storage widens exactly on write and
+   rounds on read.  Reading leaves the pads and levels 0 and nz untouched.  Files are
+   created when missing and not truncated.  A missing or short input file gives
+   OBL_ERR_IO.
+   vel_tt: the OBL_VEL_TT_FIELDS fields u, v, w, RHSx, RHSy, RHSz, Cs_opt2, F_LM, F_MM,
+   F_QN, F_NN, one after the other, in the file path_restart + "vel_tt%08d.out" (the path
+   keeps its own trailing '/'); a NULL field is written as zeros and skipped on reading.
+   checkpoint_final creates the directory path_restart when it is missing.
+   total_time.dat holds the step number nums as one list-directed integer; reading a
+   missing file gives nums = 0 and OBL_OK, as the reference starts from step 0. */
+#define OBL_VEL_TT_FIELDS 11
+int obl_write_file_3d_dev(obl_ctx *ctx, const void *var, const char *fn, long long disp0, int zrank, int nzranks);
+int obl_read_file_3d_dev(obl_ctx *ctx, void *var, const char *fn, long long disp0, int zrank, int nzranks);
+int obl_checkpoint_final_dev(obl_ctx *ctx, const char *path_restart, int nums, const void *const *fields, int zrank,
+                             int nzranks);
+int obl_read_flow_field_dev(obl_ctx *ctx, const char *path_restart, int nums, void *const *fields, int zrank,
+                            int nzranks);
+int obl_read_total_time(const char *fn, int *nums);
+int obl_write_total_time(const char *fn, int nums);
 
 /* ---- 2D transforms fftn_mpi / ifftn_mpi (203_fftn_mpi.f90:4-35, 39-67) ----
    in (ldx, nyt, nlev) real -> out (lhx, nyt, nlev) complex, unnormalised, x- and

@@ -25,7 +25,9 @@ LIB_PATH = os.environ.get("OBL_LIB") or os.path.join(_HERE, "libobl_b200.so")
 
 OBL_OK = 0
 ERRORS = {1: "OBL_ERR_ARG", 2: "OBL_ERR_CUDA", 3: "OBL_ERR_NOMEM", 4: "OBL_ERR_TIMEOUT",
-          5: "OBL_ERR_UNSUPPORTED", 6: "OBL_ERR_NODEV"}
+          5: "OBL_ERR_UNSUPPORTED", 6: "OBL_ERR_NODEV", 7: "OBL_ERR_IO"}
+# the fields of a vel_tt restart file, in file order (012_io.f90:526-546)
+VEL_TT_FIELDS = ("u", "v", "w", "RHSx", "RHSy", "RHSz", "Cs_opt2", "F_LM", "F_MM", "F_QN", "F_NN")
 PRECISION = {"f64": 0, "mixed": 1, "f32": 2}
 TOP_BC = {"single": 0, "neumann": 1}
 
@@ -37,6 +39,8 @@ EXPORTS = [
     "obl_ddx", "obl_ddy", "obl_ddx_dev", "obl_ddy_dev",
     "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
     "obl_divstress_uv", "obl_divstress_w", "obl_divstress_uv_dev", "obl_divstress_w_dev",
+    "obl_write_file_3d_dev", "obl_read_file_3d_dev", "obl_checkpoint_final_dev", "obl_read_flow_field_dev",
+    "obl_read_total_time", "obl_write_total_time",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
     "obl_zero_padding", "obl_zero_unpadding", "obl_zero_padding_dev", "obl_zero_unpadding_dev",
     "obl_zero_padding_noalloc_dev",
@@ -119,6 +123,12 @@ def load_library(path=LIB_PATH):
         "obl_ddz_uv_dev": [ctx, P, P], "obl_ddz_w_dev": [ctx, P, P],
         "obl_divstress_uv": [ctx, P, P, P, P], "obl_divstress_w": [ctx, P, P, P, P],
         "obl_divstress_uv_dev": [ctx, P, P, P, P], "obl_divstress_w_dev": [ctx, P, P, P, P],
+        "obl_write_file_3d_dev": [ctx, P, ctypes.c_char_p, ctypes.c_longlong, I, I],
+        "obl_read_file_3d_dev": [ctx, P, ctypes.c_char_p, ctypes.c_longlong, I, I],
+        "obl_checkpoint_final_dev": [ctx, ctypes.c_char_p, I, ctypes.POINTER(P), I, I],
+        "obl_read_flow_field_dev": [ctx, ctypes.c_char_p, I, ctypes.POINTER(P), I, I],
+        "obl_read_total_time": [ctypes.c_char_p, ctypes.POINTER(I)],
+        "obl_write_total_time": [ctypes.c_char_p, I],
         "obl_fftn": [ctx, P, P, I], "obl_ifftn": [ctx, P, P, I],
         "obl_fftn_dev": [ctx, P, P, I], "obl_ifftn_dev": [ctx, P, P, I],
         "obl_zero_padding": [ctx, P, P, I], "obl_zero_unpadding": [ctx, P, P, I],
@@ -376,6 +386,39 @@ class Context:
     def ddz_w_dev(self, dfdz, fun):
         self._check(self._lib.obl_ddz_w_dev(self._h, dfdz, fun), "ddz_w_dev")
 
+    # ---- restart files (integer device pointers; FP64 files, see include/obl.h) ----
+    def write_file_3d_dev(self, var, fn, disp0=0, zrank=0, nzranks=1):
+        """write_file_mpi_3d (202_parallel.f90:1084-1120): levels 1..nz-1 of var."""
+        self._check(self._lib.obl_write_file_3d_dev(self._h, var, os.fsencode(fn), disp0, zrank, nzranks),
+                    "write_file_3d_dev")
+
+    def read_file_3d_dev(self, var, fn, disp0=0, zrank=0, nzranks=1):
+        """read_file_mpi_3d (202_parallel.f90:1211-1250): levels 1..nz-1 of var."""
+        self._check(self._lib.obl_read_file_3d_dev(self._h, var, os.fsencode(fn), disp0, zrank, nzranks),
+                    "read_file_3d_dev")
+
+    @staticmethod
+    def _vel_tt_ptrs(fields):
+        if isinstance(fields, dict):
+            fields = [fields.get(k) for k in VEL_TT_FIELDS]
+        fields = list(fields)
+        if len(fields) != len(VEL_TT_FIELDS):
+            raise ValueError(f"vel_tt holds {len(VEL_TT_FIELDS)} fields {VEL_TT_FIELDS}")
+        return (ctypes.c_void_p * len(fields))(*[f if f else None for f in fields])
+
+    def checkpoint_final_dev(self, path_restart, nums, fields, zrank=0, nzranks=1):
+        """checkpoint_final (012_io.f90:496-546): vel_tt%08d.out from device fields (a list
+        in VEL_TT_FIELDS order or a dict by name; missing fields are written as zeros)."""
+        self._check(self._lib.obl_checkpoint_final_dev(self._h, os.fsencode(path_restart), nums,
+                                                       self._vel_tt_ptrs(fields), zrank, nzranks),
+                    "checkpoint_final_dev")
+
+    def read_flow_field_dev(self, path_restart, nums, fields, zrank=0, nzranks=1):
+        """read_flow_field (102_01_ic.f90:682-734) into device fields (missing ones skipped)."""
+        self._check(self._lib.obl_read_flow_field_dev(self._h, os.fsencode(path_restart), nums,
+                                                      self._vel_tt_ptrs(fields), zrank, nzranks),
+                    "read_flow_field_dev")
+
     def divstress_uv_dev(self, divt, tx, ty, tz):
         self._check(self._lib.obl_divstress_uv_dev(self._h, divt, tx, ty, tz), "divstress_uv_dev")
 
@@ -497,6 +540,23 @@ class Context:
                                                    float(z_hi), ctypes.byref(J), gu, gv, gw),
                     "rollout_grad_dev")
         return J.value
+
+
+def read_total_time(fn):
+    """The step number of total_time.dat (0 when the file is missing, as the reference)."""
+    L = load_library()
+    n = ctypes.c_int(0)
+    rc = L.obl_read_total_time(os.fsencode(fn), ctypes.byref(n))
+    if rc:
+        raise OblError(f"read_total_time({fn}): {ERRORS.get(rc, rc)}")
+    return n.value
+
+
+def write_total_time(fn, nums):
+    """total_time.dat as the reference writes it (one list-directed integer)."""
+    rc = load_library().obl_write_total_time(os.fsencode(fn), int(nums))
+    if rc:
+        raise OblError(f"write_total_time({fn}): {ERRORS.get(rc, rc)}")
 
 
 def stepio_dev(u, v, w, theta, d, big, p, dp, divtz_bot=None, divtz_top=None):

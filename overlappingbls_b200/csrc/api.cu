@@ -4,12 +4,18 @@
 // init_parameter / init_fft_plan / init_wavenumber / init_coef_press (tables are built
 // once: twiddles w_N^m in the storage precision, kx/ky wavenumbers in FP64, the FP64
 // island list of the mixed mode) and owns the device work buffers.
+#include <cerrno>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "common.cuh"
 #include "lines.cuh"
@@ -19,6 +25,7 @@
 #include "ensemble.cuh"
 #include "slab.cuh"
 #include "divstress.cuh"
+#include "restart.cuh"
 
 using namespace obl;
 
@@ -67,6 +74,7 @@ struct obl_ctx {
     // z-slab solve: particular solution, spikes, modified upper band; bulk columns in the
     // storage type, FP64 island columns of the mixed mode apart
     DevBuf slab_v, slab_cp;
+    IoStage io;                  // restart-file chunks (two device, two pinned host)
     DevBuf slab_iy, slab_iv, slab_icp;
     // tuning parameters (obl_set_param)
     long long param_fused = 0;          // use the cluster-fused kernels in obl_step
@@ -422,6 +430,23 @@ template <typename T> struct Ops {
         LaunchScope ls(ctx->rec, "ddz_w", s());
         launch_ddz_w<T>(d, f, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->dz, s(), e);
         return chk(e, "ddz_w");
+    }
+
+    // ---- restart files (202_parallel.f90:1084-1250): levels 1..nz-1 of one field ----
+    int io_reserve()
+    {
+        const size_t plane = (size_t)ctx->nxt * ctx->nyt, chunk = (size_t)8 << 20;   // 64 MiB of doubles
+        return io_stage_reserve(ctx->io, chunk > plane ? chunk : plane, ctx->err);
+    }
+    int write_field(const T *var, int fd, long long off)
+    {
+        int rc = io_reserve();
+        return rc ? rc : io_write_field<T>(ctx->io, s(), fd, off, var, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->err);
+    }
+    int read_field(T *var, int fd, long long off)
+    {
+        int rc = io_reserve();
+        return rc ? rc : io_read_field<T>(ctx->io, s(), fd, off, var, ctx->nxt, ctx->ldx, ctx->nyt, ctx->nz, ctx->err);
     }
 
     // ---- divstress_uv / divstress_w (107_divstress.f90:4-104), single-rank roles ----
@@ -1215,6 +1240,7 @@ int obl_ctx_destroy(obl_ctx *ctx)
     for (auto &b : ctx->rw_big) cudaFree(b.p);
     cudaFree(ctx->ckpt.p);
     cudaFree(ctx->ke.p);
+    io_stage_free(ctx->io);
     cudaFree(ctx->slab_v.p);
     cudaFree(ctx->slab_cp.p);
     cudaFree(ctx->slab_iy.p);
@@ -1360,6 +1386,54 @@ template <class F> static int dispatchT(obl_ctx *ctx, F fn)
 
 static bool nlev_ok(const obl_ctx *c, int nlev) { return nlev > 0 && ((long long)c->nyt * nlev) % 2 == 0; }
 
+// ---- restart files ----
+namespace {
+struct Fd {
+    int fd = -1;
+    ~Fd()
+    {
+        if (fd >= 0) close(fd);
+    }
+};
+// bytes of one field in the file: the global (nxt, nyt, nzranks*(nz-1)) FP64 array
+long long io_field_bytes(const obl_ctx *c, int nzranks)
+{
+    return (long long)c->nxt * c->nyt * (c->nz - 1) * nzranks * (long long)sizeof(double);
+}
+// byte offset of this rank's z-block inside a field (subarray start (nz-1)*coordz)
+long long io_rank_off(const obl_ctx *c, int zrank)
+{
+    return (long long)c->nxt * c->nyt * (c->nz - 1) * zrank * (long long)sizeof(double);
+}
+bool io_ranks_ok(int zrank, int nzranks) { return nzranks >= 1 && zrank >= 0 && zrank < nzranks; }
+std::string vel_tt_name(const char *path_restart, int nums)
+{
+    char b[32];
+    std::snprintf(b, sizeof b, "vel_tt%08d.out", nums);   // 012_io.f90:524, 102_01_ic.f90:711
+    return std::string(path_restart) + b;
+}
+template <class F> int io_call(obl_ctx *ctx, F fn)
+{
+    if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice");
+    return dispatchT(ctx, [&](auto &o) -> int {
+        using T = typename std::remove_reference<decltype(o)>::type::Tt;
+        return fn(o, (T *)nullptr);
+    });
+}
+int open_out(obl_ctx *ctx, const std::string &fn, Fd &f)
+{
+    f.fd = open(fn.c_str(), O_WRONLY | O_CREAT, 0644);   // MPI_MODE_WRONLY+MPI_MODE_CREATE: no truncation
+    if (f.fd < 0) return fail(ctx, OBL_ERR_IO, "open " + fn + ": " + std::strerror(errno));
+    return OBL_OK;
+}
+int open_in(obl_ctx *ctx, const std::string &fn, Fd &f)
+{
+    f.fd = open(fn.c_str(), O_RDONLY);
+    if (f.fd < 0) return fail(ctx, OBL_ERR_IO, "FILE DOES NOT EXIST: " + fn);   // 202_parallel.f90:1244-1246
+    return OBL_OK;
+}
+} // namespace
+
 extern "C" {
 
 int obl_ddx_dev(obl_ctx *ctx, void *dfdx, const void *fun, int nlev)
@@ -1387,6 +1461,96 @@ int obl_divstress_w_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty
     if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2) return OBL_ERR_ARG;
     DEVCALL(ctx, return o.divstress((T *)divt, (const T *)tx, (const T *)ty, (const T *)tz, true););
 }
+
+int obl_write_file_3d_dev(obl_ctx *ctx, const void *var, const char *fn, long long disp0, int zrank, int nzranks)
+{
+    if (!ctx || !var || !fn || disp0 < 0 || !io_ranks_ok(zrank, nzranks) || ctx->nz < 2) return OBL_ERR_ARG;
+    Fd f;
+    int rc = open_out(ctx, fn, f);
+    if (rc) return rc;
+    return io_call(ctx, [&](auto &o, auto *tp) -> int {
+        using T = typename std::remove_pointer<decltype(tp)>::type;
+        return o.write_field((const T *)var, f.fd, disp0 + io_rank_off(ctx, zrank));
+    });
+}
+int obl_read_file_3d_dev(obl_ctx *ctx, void *var, const char *fn, long long disp0, int zrank, int nzranks)
+{
+    if (!ctx || !var || !fn || disp0 < 0 || !io_ranks_ok(zrank, nzranks) || ctx->nz < 2) return OBL_ERR_ARG;
+    Fd f;
+    int rc = open_in(ctx, fn, f);
+    if (rc) return rc;
+    return io_call(ctx, [&](auto &o, auto *tp) -> int {
+        using T = typename std::remove_pointer<decltype(tp)>::type;
+        return o.read_field((T *)var, f.fd, disp0 + io_rank_off(ctx, zrank));
+    });
+}
+int obl_checkpoint_final_dev(obl_ctx *ctx, const char *path_restart, int nums, const void *const *fields, int zrank,
+                             int nzranks)
+{
+    if (!ctx || !path_restart || !fields || nums < 0 || !io_ranks_ok(zrank, nzranks) || ctx->nz < 2)
+        return OBL_ERR_ARG;
+    // the restart directory is created when missing (012_io.f90:514-518)
+    struct stat st;
+    if (path_restart[0] && stat(path_restart, &st) != 0 && mkdir(path_restart, 0755) != 0 && errno != EEXIST)
+        return fail(ctx, OBL_ERR_IO, std::string("mkdir ") + path_restart + ": " + std::strerror(errno));
+    Fd f;
+    const std::string fn = vel_tt_name(path_restart, nums);
+    int rc = open_out(ctx, fn, f);
+    if (rc) return rc;
+    const long long disp3d = io_field_bytes(ctx, nzranks), roff = io_rank_off(ctx, zrank);
+    return io_call(ctx, [&](auto &o, auto *tp) -> int {
+        using T = typename std::remove_pointer<decltype(tp)>::type;
+        for (int k = 0; k < OBL_VEL_TT_FIELDS; ++k) {   // 012_io.f90:526-546
+            int r = o.write_field((const T *)fields[k], f.fd, k * disp3d + roff);
+            if (r) return r;
+        }
+        return OBL_OK;
+    });
+}
+int obl_read_flow_field_dev(obl_ctx *ctx, const char *path_restart, int nums, void *const *fields, int zrank,
+                            int nzranks)
+{
+    if (!ctx || !path_restart || !fields || nums < 0 || !io_ranks_ok(zrank, nzranks) || ctx->nz < 2)
+        return OBL_ERR_ARG;
+    Fd f;
+    int rc = open_in(ctx, vel_tt_name(path_restart, nums), f);
+    if (rc) return rc;
+    const long long disp3d = io_field_bytes(ctx, nzranks), roff = io_rank_off(ctx, zrank);
+    return io_call(ctx, [&](auto &o, auto *tp) -> int {
+        using T = typename std::remove_pointer<decltype(tp)>::type;
+        for (int k = 0; k < OBL_VEL_TT_FIELDS; ++k) {   // 102_01_ic.f90:713-733
+            if (!fields[k]) continue;
+            int r = o.read_field((T *)fields[k], f.fd, k * disp3d + roff);
+            if (r) return r;
+        }
+        return OBL_OK;
+    });
+}
+int obl_read_total_time(const char *fn, int *nums)
+{
+    if (!fn || !nums) return OBL_ERR_ARG;
+    FILE *fp = std::fopen(fn, "r");
+    if (!fp) {   // "Restart file NOT found": the run starts from step 0 (102_01_ic.f90:699-705)
+        *nums = 0;
+        return OBL_OK;
+    }
+    long long v = 0;
+    const int got = std::fscanf(fp, "%lld", &v);   // list-directed read of one integer
+    std::fclose(fp);
+    if (got != 1 || v < 0 || v > 2147483647LL) return OBL_ERR_IO;
+    *nums = (int)v;
+    return OBL_OK;
+}
+int obl_write_total_time(const char *fn, int nums)
+{
+    if (!fn || nums < 0) return OBL_ERR_ARG;
+    FILE *fp = std::fopen(fn, "w");
+    if (!fp) return OBL_ERR_IO;
+    // list-directed write of a default integer: right-aligned in 12 columns (012_io.f90:487-489)
+    const int ok = std::fprintf(fp, "%12d\n", nums) > 0;
+    return (std::fclose(fp) == 0 && ok) ? OBL_OK : OBL_ERR_IO;
+}
+
 int obl_ddz_w_dev(obl_ctx *ctx, void *dfdz, const void *fun)
 {
     if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
