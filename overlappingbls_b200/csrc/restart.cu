@@ -151,8 +151,10 @@ int io_write_field(IoStage &s, cudaStream_t st, int fd, long long off, const T *
             const int nl = (L - p * per) < per ? (L - p * per) : per;
             if ((e = cudaEventSynchronize(s.ev[p & 1])) != cudaSuccess) return cu_err(err, e, "restart copy");
             if ((rc = write_all(fd, s.host[p & 1], (size_t)(plane * nl) * sizeof(double),
-                                off + (long long)p * per * plane * (long long)sizeof(double), err)))
+                                off + (long long)p * per * plane * (long long)sizeof(double), err))) {
+                cudaStreamSynchronize(st);   // nothing may still copy into the pinned chunks
                 return rc;
+            }
         }
     }
     return OBL_OK;
@@ -187,8 +189,10 @@ int io_read_field(IoStage &s, cudaStream_t st, int fd, long long off, T *var, in
             const int q = c + 1;
             if (q >= 2 && (e = cudaEventSynchronize(s.ev[q & 1])) != cudaSuccess) return cu_err(err, e, "restart copy");
             if ((rc = read_all(fd, s.host[q & 1], (size_t)(plane * levels(q)) * sizeof(double),
-                               off + (long long)q * per * plane * (long long)sizeof(double), err)))
+                               off + (long long)q * per * plane * (long long)sizeof(double), err))) {
+                cudaStreamSynchronize(st);   // nothing may still copy out of the pinned chunks
                 return rc;
+            }
         }
     }
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cu_err(err, e, "restart unpack");
