@@ -98,10 +98,14 @@ long long obl_launch_count(const obl_ctx *ctx);
    {"kernel": [launches, total_ms], ...} (synchronizes; clears the records) */
 int obl_timing_enable(obl_ctx *ctx, int on);
 int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
-/* execution tuning (results do not depend on it):
+/* execution tuning (results do not depend on it beyond rounding):
      "fused"             1 = cluster-fused plane kernels in obl_step (square grids), 0 = line kernels
      "fwd_clusters"      clusters of the fused forward kernel (0 = as many as can be resident)
-     "fwd_cluster_size"  CTAs per cluster (1..16; above 8 needs non-portable cluster support) */
+     "fwd_cluster_size"  CTAs per cluster (1..16; above 8 needs non-portable cluster support)
+     "tdma_segments"     segments each (kx,ky) column of the pressure solve is split into
+                         and solved at once (0 = chosen by size: more than one only when
+                         the columns alone cannot fill the GPU; 1 = one sequential sweep;
+                         up to 16; used in the Neumann-top mode with spectral dpdz) */
 int obl_set_param(obl_ctx *ctx, const char *name, long long value);
 int obl_get_param(obl_ctx *ctx, const char *name, long long *value);
 
@@ -341,7 +345,8 @@ int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n);
         and plane_out = this rank's H_z(1) spectrum (plane_bytes);
      2. caller: all-gather the planes; plane_above = the plane of rank+1 (ignored on the
         top rank);
-     3. obl_slab_solve_dev: the rank's rows eliminated in FP64; iface_out = its interface
+     3. obl_slab_solve_dev: the rank's rows eliminated (in the storage precision, the FP64
+        island columns of the mixed mode in FP64); iface_out = its interface
         coefficients (iface_bytes, FP64);
      4. caller: all-gather the interface coefficients, rank-major (nranks * iface_bytes);
      5. obl_slab_finish_dev: the reduced 2*nranks-unknown system (redundantly), the rank's

@@ -75,11 +75,13 @@ struct obl_ctx {
     // storage type, FP64 island columns of the mixed mode apart
     DevBuf slab_v, slab_cp;
     IoStage io;                  // restart-file chunks (two device, two pinned host)
+    DevBuf seg_iface;            // interface values of the segmented single-domain solve
     DevBuf slab_iy, slab_iv, slab_icp;
     // tuning parameters (obl_set_param)
     long long param_fused = 0;          // use the cluster-fused kernels in obl_step
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
     long long param_fwd_csize = 8;      // CTAs per cluster
+    long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t ev[9] = {};
@@ -343,7 +345,33 @@ template <typename T> struct Ops {
         ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz;
         ta.dph = dpdz_out ? (C2<T> *)ctx->spec[4].p : nullptr;
         ta.neumann_top = ctx->opt.top_bc == OBL_TOP_NEUMANN;
-        {
+        const int P = (ta.neumann_top && ta.dph) ? seg_parts(S, L) : 1;
+        if (P > 1) {
+            // the columns split into segments solved at once (partitioned Thomas, as across
+            // z-ranks), then the reduced interface system and the back substitution
+            const int seg = (L + P - 1) / P, Pn = (L + seg - 1) / seg;
+            const size_t n = (size_t)S * L, ni = (size_t)(ctx->n_isl > 0 ? ctx->n_isl : 1) * L;
+            if ((rc = ensure(ctx, ctx->slab_v, sizeof(T) * n)) || (rc = ensure(ctx, ctx->slab_cp, sizeof(T) * n)) ||
+                (rc = ensure(ctx, ctx->slab_iy, sizeof(double2) * ni)) ||
+                (rc = ensure(ctx, ctx->slab_iv, sizeof(double) * ni)) ||
+                (rc = ensure(ctx, ctx->slab_icp, sizeof(double) * ni)) ||
+                (rc = ensure(ctx, ctx->seg_iface, sizeof(double) * kSlabIface * (size_t)S * Pn)))
+                return rc;
+            SlabArgs<T> a = slab_args(0, 1);
+            a.Hx = Hx; a.Hy = Hy; a.Hz = Hz; a.phat = ph; a.dph = ta.dph;
+            a.iface = (double *)ctx->seg_iface.p;
+            a.iface_all = a.iface;
+            cudaError_t e = cudaSuccess;
+            {
+                LaunchScope ls(ctx->rec, "tdma_seg_solve", s());
+                launch_seg_solve<T>(a, Pn, seg, s(), e);
+            }
+            {
+                LaunchScope ls(ctx->rec, "tdma_seg_finish", s());
+                launch_seg_finish<T>(a, Pn, seg, s(), e);
+            }
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_seg");
+        } else {
             cudaError_t e = cudaSuccess;
             if (ctx->n_isl) {
                 // FP32 bulk and FP64 island columns in one launch
@@ -811,7 +839,22 @@ template <typename T> struct Ops {
         a.kx = ctx->d_kx; a.ky = ctx->d_ky2;
         a.S = ctx->sp(); a.lhx = ctx->lhx; a.nyt = ctx->nyt; a.L = ctx->L; a.dz = ctx->dz;
         a.rank = rank; a.nranks = P;
+        a.own_p0 = 1;
         return a;
+    }
+    // Segments of the single-domain column solve: enough (kx,ky)-column segments to fill
+    // the GPU (8 resident blocks of 128 threads per SM) when the columns alone do not, at
+    // least 8 levels each; 1 = the sequential sweep.
+    int seg_parts(long long S, int L) const
+    {
+        if (ctx->param_tdma_segments > 0) return (int)std::min<long long>(ctx->param_tdma_segments, L);
+        if (S >= 65536) return 1;
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const long long want = ((long long)nsm * 8 * 128 + S - 1) / S;
+        const long long P = std::min<long long>(std::min<long long>(want, kSlabMaxRanks), L / 8);
+        return P > 1 ? (int)P : 1;
     }
     // the rank's forward pass (ddx, ddy, zero_padding of u,v,w,theta and the RHS spectra),
     // its boundary planes, and a copy of its H_z(1) plane for the rank below
@@ -1241,6 +1284,7 @@ int obl_ctx_destroy(obl_ctx *ctx)
     cudaFree(ctx->ckpt.p);
     cudaFree(ctx->ke.p);
     io_stage_free(ctx->io);
+    cudaFree(ctx->seg_iface.p);
     cudaFree(ctx->slab_v.p);
     cudaFree(ctx->slab_cp.p);
     cudaFree(ctx->slab_iy.p);
@@ -1299,6 +1343,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "fused")) return &ctx->param_fused;
     if (!std::strcmp(name, "fwd_clusters")) return &ctx->param_fwd_clusters;
     if (!std::strcmp(name, "fwd_cluster_size")) return &ctx->param_fwd_csize;
+    if (!std::strcmp(name, "tdma_segments")) return &ctx->param_tdma_segments;
     return nullptr;
 }
 
@@ -1309,6 +1354,8 @@ int obl_set_param(obl_ctx *ctx, const char *name, long long value)
     if (!p) return fail(ctx, OBL_ERR_ARG, std::string("unknown parameter ") + name);
     if (!std::strcmp(name, "fwd_cluster_size") && (value < 1 || value > 16))
         return fail(ctx, OBL_ERR_ARG, "fwd_cluster_size must be 1..16");
+    if (!std::strcmp(name, "tdma_segments") && (value < 0 || value > kSlabMaxRanks))
+        return fail(ctx, OBL_ERR_ARG, "tdma_segments must be 0..16");
     *p = value;
     return OBL_OK;
 }

@@ -95,10 +95,11 @@ __device__ __forceinline__ void slab_column(const SlabArgs<T> &a, long long t)
     if (q < 0) return;
     const long long S = a.S;
     const int L = a.L;
-    double *f = a.iface + q * kSlabIface;
+    // interface values field-major, (kSlabIface, S): each store and load is coalesced
+    auto fset = [&](int k, double v) { a.iface[(long long)k * S + q] = v; };
     const int ix = (int)(q % a.lhx), iy = (int)(q / a.lhx);
     if (ix == a.lhx - 1 || iy == a.nyt / 2) {   // Nyquist columns: p_hat = 0
-        for (int k = 0; k < kSlabIface; ++k) f[k] = 0.0;
+        for (int k = 0; k < kSlabIface; ++k) fset(k, 0.0);
         return;
     }
     const double kxd = a.kx[ix], kyd = a.ky[iy], k2d = kxd * kxd + kyd * kyd;
@@ -169,10 +170,10 @@ __device__ __forceinline__ void slab_column(const SlabArgs<T> &a, long long t)
             cprev = cpj;
         }
     }
-    f[2] = yp.x;
-    f[3] = yp.y;
-    f[5] = vp;
-    f[7] = wl;
+    fset(2, yp.x);
+    fset(3, yp.y);
+    fset(5, vp);
+    fset(7, wl);
     // ---- end values at row 1: y_j = y'_j - c'_j y_{j+1}, likewise v; w_j = -c'_j w_{j+1} ----
     CC yn = yp;
     TC vn = vp, wn = wl;
@@ -181,10 +182,10 @@ __device__ __forceinline__ void slab_column(const SlabArgs<T> &a, long long t)
         vn = v - c * vn;
         wn = -c * wn;
     });
-    f[0] = yn.x;
-    f[1] = yn.y;
-    f[4] = vn;
-    f[6] = wn;
+    fset(0, yn.x);
+    fset(1, yn.y);
+    fset(4, vn);
+    fset(6, wn);
 }
 
 // island blocks first (their FP64 sweeps are the longest), then the bulk columns
@@ -228,7 +229,7 @@ __device__ __forceinline__ void slab_rows_out(const SlabArgs<T> &a, long long q,
         const TC dz = (TC)a.dz;
         x0 = mk<TC>(xn.x - dz * (TC)h.x, xn.y - dz * (TC)h.y);
     }
-    ph[0] = mk<T>((T)x0.x, (T)x0.y);
+    if (a.own_p0) ph[0] = mk<T>((T)x0.x, (T)x0.y);
     dph[S] = mk<T>((T)((xn.x - x0.x) * rdz), (T)((xn.y - x0.y) * rdz));
 }
 
@@ -243,7 +244,7 @@ __device__ __forceinline__ void slab_finish_column(const SlabArgs<T> &a, long lo
     const int ix = (int)(q % a.lhx), iy = (int)(q / a.lhx);
     C2<T> *ph = a.phat + q, *dph = a.dph + q;
     if (ix == a.lhx - 1 || iy == a.nyt / 2) {
-        for (int z = 0; z <= L; ++z) ph[S * z] = mk<T>(0, 0);
+        for (int z = a.own_p0 ? 0 : 1; z <= L; ++z) ph[S * z] = mk<T>(0, 0);
         for (int z = 1; z <= L; ++z) dph[S * z] = mk<T>(0, 0);
         return;
     }
@@ -252,37 +253,50 @@ __device__ __forceinline__ void slab_finish_column(const SlabArgs<T> &a, long lo
     // upward from rank 0, X_k = Z_k - G_k X_{k+1}, where G_k has only a first column (g0, g1);
     // downward from rank P-1, X_k = Z'_k - H_k X_{k-1}, where H_k has only a second column
     // (h0, h1); the two meet at this rank's own 2x2 block.
-    auto iface = [&](int k) { return a.iface_all + ((long long)k * S + q) * kSlabIface; };
+    // rank k's record of this column; the next record's loads are issued before the
+    // current one is used
+    auto rec = [&](int k, double *f) {
+#pragma unroll
+        for (int j = 0; j < kSlabIface; ++j) f[j] = a.iface_all[((long long)k * kSlabIface + j) * S + q];
+    };
+    double cur[kSlabIface], nxt[kSlabIface];
     double g1 = 0.0;
     double2 z1 = make_double2(0.0, 0.0);   // last_{r-1} = z1 - g1 first_r
+    if (r > 0) rec(0, cur);
     for (int k = 0; k < r; ++k) {
-        const double *f = iface(k);
-        const double v1 = f[4], vm = f[5], w1 = f[6], wm = f[7];
+        if (k + 1 < r) rec(k + 1, nxt);
+        const double v1 = cur[4], vm = cur[5], w1 = cur[6], wm = cur[7];
         // D = I - A_k G_{k-1} = [[1 - v1 g1, 0], [-vm g1, 1]]; rhs = Y_k - A_k Z_{k-1}
         const double d00 = 1.0 - v1 * g1, d10 = -vm * g1;
-        const double2 r0 = make_double2(f[0] - v1 * z1.x, f[1] - v1 * z1.y);
-        const double2 r1 = make_double2(f[2] - vm * z1.x, f[3] - vm * z1.y);
+        const double2 r0 = make_double2(cur[0] - v1 * z1.x, cur[1] - v1 * z1.y);
+        const double2 r1 = make_double2(cur[2] - vm * z1.x, cur[3] - vm * z1.y);
         const double i00 = 1.0 / d00;
         const double2 zz0 = make_double2(r0.x * i00, r0.y * i00);
         z1 = make_double2(r1.x - d10 * zz0.x, r1.y - d10 * zz0.y);
         g1 = wm - d10 * (w1 * i00);
+#pragma unroll
+        for (int j = 0; j < kSlabIface; ++j) cur[j] = nxt[j];
     }
     double h0 = 0.0;
     double2 z0 = make_double2(0.0, 0.0);   // first_{r+1} = z0 - h0 last_r
+    if (r < P - 1) rec(P - 1, cur);
     for (int k = P - 1; k > r; --k) {
-        const double *f = iface(k);
-        const double v1 = f[4], vm = f[5], w1 = f[6], wm = f[7];
+        if (k - 1 > r) rec(k - 1, nxt);
+        const double v1 = cur[4], vm = cur[5], w1 = cur[6], wm = cur[7];
         // D' = I - C_k H_{k+1} = [[1, -w1 h0], [0, 1 - wm h0]]; rhs = Y_k - C_k Z'_{k+1}
         const double d01 = -w1 * h0, d11 = 1.0 - wm * h0;
-        const double2 r0 = make_double2(f[0] - w1 * z0.x, f[1] - w1 * z0.y);
-        const double2 r1 = make_double2(f[2] - wm * z0.x, f[3] - wm * z0.y);
+        const double2 r0 = make_double2(cur[0] - w1 * z0.x, cur[1] - w1 * z0.y);
+        const double2 r1 = make_double2(cur[2] - wm * z0.x, cur[3] - wm * z0.y);
         const double i11 = 1.0 / d11;
         const double2 zz1 = make_double2(r1.x * i11, r1.y * i11);
         z0 = make_double2(r0.x - d01 * zz1.x, r0.y - d01 * zz1.y);
         h0 = v1 - d01 * (vm * i11);
+#pragma unroll
+        for (int j = 0; j < kSlabIface; ++j) cur[j] = nxt[j];
     }
     // the rank's own block with both neighbours substituted
-    const double *f = iface(r);
+    double f[kSlabIface];
+    rec(r, f);
     const double v1 = f[4], vm = f[5], w1 = f[6], wm = f[7];
     const double m00 = 1.0 - v1 * g1, m01 = -w1 * h0, m10 = -vm * g1, m11 = 1.0 - wm * h0;
     const double2 c0 = make_double2(f[0] - v1 * z1.x - w1 * z0.x, f[1] - v1 * z1.y - w1 * z0.y);
@@ -303,6 +317,50 @@ __global__ void __launch_bounds__(128, OBL_SLAB_MINB) k_slab_finish(SlabArgs<T> 
         slab_finish_column<T, double, true>(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
     else
         slab_finish_column<T, T, false>(a, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
+}
+
+// Segment r of a column split on one GPU: the segment's view of the whole column's arguments.
+template <typename T> __device__ __forceinline__ SlabArgs<T> seg_view(const SlabArgs<T> &a, int r, int P, int seg)
+{
+    SlabArgs<T> b = a;
+    const long long off = (long long)r * seg * a.S, ioff = (long long)r * seg * a.n_isl;
+    b.Hx = a.Hx + off;
+    b.Hy = a.Hy + off;
+    b.Hz = a.Hz + off;
+    b.phat = a.phat + off;
+    b.dph = a.dph + off;
+    b.v = a.v + off;
+    b.cp = a.cp + off;
+    b.iy = a.iy + ioff;
+    b.iv = a.iv + ioff;
+    b.icp = a.icp + ioff;
+    b.iface = a.iface + (long long)r * a.S * kSlabIface;
+    b.iface_all = a.iface;
+    b.rank = r;
+    b.nranks = P;
+    b.L = (a.L - r * seg) < seg ? (a.L - r * seg) : seg;
+    b.own_p0 = r == 0;
+    return b;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128, OBL_SLAB_MINB) k_seg_solve(SlabArgs<T> a, int nbi, int seg)
+{
+    const SlabArgs<T> b = seg_view(a, blockIdx.y, gridDim.y, seg);
+    if ((int)blockIdx.x < nbi)
+        slab_column<T, double, true>(b, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    else
+        slab_column<T, T, false>(b, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128, OBL_SLAB_MINB) k_seg_finish(SlabArgs<T> a, int nbi, int seg)
+{
+    const SlabArgs<T> b = seg_view(a, blockIdx.y, gridDim.y, seg);
+    if ((int)blockIdx.x < nbi)
+        slab_finish_column<T, double, true>(b, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    else
+        slab_finish_column<T, T, false>(b, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
@@ -339,6 +397,20 @@ template <typename T> void launch_slab_finish(const SlabArgs<T> &a, cudaStream_t
     k_slab_finish<T><<<(unsigned)(nbi + nbb), 128, 0, s>>>(a, nbi);
     e = cudaGetLastError();
 }
+template <typename T> void launch_seg_solve(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    const int nbi = (a.n_isl + 127) / 128, nbb = (int)((a.S + 127) / 128);
+    k_seg_solve<T><<<dim3((unsigned)(nbi + nbb), (unsigned)P), 128, 0, s>>>(a, nbi, seg);
+    e = cudaGetLastError();
+}
+template <typename T> void launch_seg_finish(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    const int nbi = (a.n_isl + 127) / 128, nbb = (int)((a.S + 127) / 128);
+    k_seg_finish<T><<<dim3((unsigned)(nbi + nbb), (unsigned)P), 128, 0, s>>>(a, nbi, seg);
+    e = cudaGetLastError();
+}
 template <typename T>
 void launch_project_bc_roles(T *u, T *v, T *w, int ldx, int nyt, int nz, int stress_free, int bottom, int top,
                              cudaStream_t s, cudaError_t &e)
@@ -351,6 +423,8 @@ void launch_project_bc_roles(T *u, T *v, T *w, int ldx, int nyt, int nz, int str
 #define OBL_INST(T)                                                                                      \
     template void launch_slab_solve<T>(const SlabArgs<T> &, cudaStream_t, cudaError_t &);              \
     template void launch_slab_finish<T>(const SlabArgs<T> &, cudaStream_t, cudaError_t &);             \
+    template void launch_seg_solve<T>(const SlabArgs<T> &, int, int, cudaStream_t, cudaError_t &);     \
+    template void launch_seg_finish<T>(const SlabArgs<T> &, int, int, cudaStream_t, cudaError_t &);    \
     template void launch_project_bc_roles<T>(T *, T *, T *, int, int, int, int, int, int, cudaStream_t,   \
                                              cudaError_t &);
 OBL_INST(float)

@@ -38,14 +38,23 @@ template <typename T> struct SlabArgs {
     int n_isl;
     double2 *iy;
     double *iv, *icp;
-    double *iface;              // out (solve): (S, kSlabIface)
-    const double *iface_all;    // in (finish): (P, S, kSlabIface)
+    double *iface;              // out (solve): (kSlabIface, S), field-major
+    const double *iface_all;    // in (finish): (P, kSlabIface, S)
     const double *kx, *ky;      // kx(lhx), ky_2d row (nyt), Nyquist entries 0
     long long S;
     int lhx, nyt, L;
     double dz;
     int rank, nranks;
+    int own_p0;                 // finish writes p_hat level 0 (off for the upper segments of
+                                // a column split on one GPU, whose level 0 is the segment below's)
 };
+
+// The same solve on one GPU with each column split into P segments of seg levels (the last
+// one shorter), solved at once: a = the whole column's arguments (L = all levels, rank 0 of
+// 1), scratch (S, L) and (n_isl, L), iface (P, S, kSlabIface).  For grids with too few
+// (kx,ky) columns to fill the GPU with one sequential sweep each.
+template <typename T> void launch_seg_solve(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e);
+template <typename T> void launch_seg_finish(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e);
 
 template <typename T> void launch_slab_solve(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e);
 template <typename T> void launch_slab_finish(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e);

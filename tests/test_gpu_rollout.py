@@ -202,3 +202,32 @@ def test_config3_gradient_vs_oracle(orc, config3):
           + ", ".join(f"{e:.3e}" for e in errs))
     assert abs(J - Jr) <= 1e-12 * abs(Jr)
     assert max(errs) <= 1e-10
+
+
+@pytest.mark.parametrize("prec", ["mixed", "f64"])
+def test_config3_timing(prec):
+    """Device time of one forward rollout + gradient (128^3, 16 steps, a checkpoint per
+    step), from the state on the device; CUDA events on the library's stream."""
+    import torch
+    nx, ny, nzt = C3["nx"], C3["ny"], C3["nzt"]
+    ctx = _ctx(nx, ny, nzt, prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    s = [torch.from_numpy(a.ravel(order="F")).to("cuda", dt) for a in _state(nx, ny, nzt, prec)]
+    g = [torch.zeros_like(s[0]) for _ in range(3)]
+    P = lambda t: t.data_ptr()
+    run = lambda: ctx.rollout_grad_dev(C3["nsteps"], *[P(t) for t in s], C3["z_lo"], C3["z_hi"], *[P(t) for t in g])
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    pts = nx * ny * (nzt - 1)
+    print(f"config3 {prec}: forward + gradient over {C3['nsteps']} steps {ms:.2f} ms, "
+          f"{C3['nsteps'] * pts / ms / 1e3:.0f} Mpts/s per (step + transposed step)")
+    ctx.close()

@@ -57,3 +57,34 @@ def test_step_f32_host_arrays(orc, prec):
     ctx.step(u32, v32, w32, f["theta"].astype(np.float32, order="F"), d32, big32, p32, dp32)
     assert rel_l2(p32[:nx], p[:nx]) < 1e-5
     assert rel_l2(w32, w64) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("nx,nzt", [(64, 34), (128, 129)])
+def test_step_column_segments(orc, prec, nx, nzt):
+    """The pressure solve with each (kx,ky) column split into segments solved at once
+    (partitioned Thomas on one GPU; chosen by size, or forced) against the one-sweep solve
+    and the oracle; 33 levels do not divide evenly into 3 or 16 segments."""
+    g = orc.Grid(nx, nx, nzt, **fields.DOMAIN)
+    f = identical_inputs(fields.make_fields(nx, nx, nzt), prec)
+    L = g.nz - 1
+    # the oracle's rank emulation needs whole levels per rank; every npz >= 2 is the same
+    ref = g.step(f["u"], f["v"], f["w"], f["theta"], npz=2 if L % 2 == 0 else 3)
+    outs = {}
+    for segs in (1, 0, 3, 16):
+        ctx = obl.Context(nx, nx, nzt, precision=prec, top_bc="neumann", **fields.DOMAIN)
+        ctx.set_param("tdma_segments", segs)
+        u, v, w = (f[k].copy(order="F") for k in "uvw")
+        d, big, p, dp = _alloc_step(ctx)
+        ctx.step(u, v, w, f["theta"], d, big, p, dp)
+        assert rel_l2(p[:nx, :, : L + 1], ref["p"][:nx, :, : L + 1]) < TOL[prec], segs
+        for a, k in zip(dp, ("dpdx", "dpdy", "dpdz")):
+            assert rel_l2(a[:nx, :, :L], ref[k][:nx, :, :L]) < TOL[prec], (segs, k)
+        for a, k in ((u, "u"), (v, "v"), (w, "w")):
+            assert rel_l2(a, ref[k]) < TOL[prec], (segs, k)
+        outs[segs] = (p, w)
+        ctx.close()
+    tol = 1e-12 if prec == "f64" else 2e-6
+    for segs in (0, 3, 16):
+        assert rel_l2(outs[segs][0][:nx, :, : L + 1], outs[1][0][:nx, :, : L + 1]) < tol, segs
+        assert rel_l2(outs[segs][1], outs[1][1]) < tol, segs
