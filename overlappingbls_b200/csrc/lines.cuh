@@ -55,6 +55,8 @@ template <typename T> struct ColArgs {
     int pad_copy;                    // UNPAD: also write columns 0,1 into ncols, ncols+1
     int zero_nyq;                    // FWD: zero the Nyquist row (203_fftn_mpi.f90:33)
     int kmul;                        // INV: 0 none, 1 multiply by i*kx(col), 2 by i*ky(row)
+    int pf_ahead;                    // the unit of plane z also prefetches its input lines of
+                                     // plane z + pf_ahead into L2 (0 = none)
 };
 
 // ----------------------------------------------------------------------------- configuration
@@ -528,6 +530,9 @@ template <typename T, int NW_ = 8, int WB_ = (sizeof(T) == 4 ? 8 : 4)> struct Lm
 #ifndef OBL_PAD_WB
 #define OBL_PAD_WB 8
 #endif
+#ifndef OBL_COL_PF
+#define OBL_COL_PF 2   // y-pad column kernel: L2 prefetch distance in quarters of a residency window (0 = off)
+#endif
 template <typename T, int N, int OP> constexpr int col_warps()
 {
     return (sizeof(T) == 4 && N >= 256) ? (OP == OP_PAD ? OBL_PAD_NW
@@ -620,6 +625,24 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
                 v[b * D::RF0 + r] = x;
             }
         }
+#if OBL_COL_PF
+        // the CTA that processes this line group pf_ahead planes later (about one
+        // residency window of CTAs) finds its input in L2
+        if (a.pf_ahead > 0 && act && z + a.pf_ahead < a.nlev) {
+            const E *pz = srcz + (long long)a.pf_ahead * a.src_plane;
+#pragma unroll
+            for (int b = 0; b < GG::PER; ++b) {
+                const int j = t + LL * b;
+                if (GG::FULL || j < GG::NB)
+#pragma unroll
+                    for (int r = 0; r < D::RF0; ++r) {
+                        const long long i = j + r * GG::NB;
+                        const E *ptr = pz + i * a.src_row + (REAL ? 2 * glc : glc);
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+                    }
+            }
+        }
+#endif
         if constexpr (!std::is_same<EPI, NoColEpi>::value) {
             using GP = Geo<NO, D::RBL, LL>;
             if (act) {
@@ -768,9 +791,10 @@ template <typename T, int N, int OP, int WB = LmGeo<T>::WB> inline size_t cols2_
     return sizeof(C2<T>) * ((size_t)D::TF + D::TB + (size_t)D::NM * WB);
 }
 
-template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const ColArgs<T> &a, cudaStream_t s)
+template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const ColArgs<T> &a0, cudaStream_t s)
 {
     static bool init = false;
+    static int resident = 0;   // CTAs of this kernel resident on the whole GPU
     constexpr int NW = col_warps<T, N, OP>(), WB = col_lines<T, N, OP>();
     constexpr bool TWG = col_tw_global<T, N, OP>();
     using D = LineDerived<N, OP>;
@@ -779,10 +803,18 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
     if (!init) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
+        int dev = 0, nsm = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * NW, sm);
+        resident = nsm * (per > 0 ? per : 1);
         init = true;
     }
+    ColArgs<T> a = a0;
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
     dim3 grid((nlines + WB - 1) / WB, a.nlev);
+    // y-pad only: measured 5% faster at 512x512x256; ddy and the y-transform did not gain
+    if (OBL_COL_PF && OP == OP_PAD) a.pf_ahead = (int)((OBL_COL_PF * (long long)resident + 4LL * grid.x - 1) / (4LL * grid.x));
     if (grid.x < 1 || grid.y < 1) return cudaSuccess;
     kern<<<grid, 32 * NW, sm, s>>>(a);
     return cudaGetLastError();
