@@ -7,15 +7,28 @@
 
 namespace obl {
 
-static inline dim3 sgrid(int ld, int ny, int nlev) { return dim3((ld + 127) / 128, ny, nlev); }
+// Every streaming kernel covers one level per grid row (blockIdx.y) and strides over the
+// level's (x, y) plane, 4 elements per thread: a 128^3 level is about 17 blocks instead of
+// one block per (x-tile, y), whose scheduling cost exceeded the work.
+static inline dim3 sgrid(int ld, int ny, int nlev)
+{
+    const long long n = (long long)ld * ny;
+    return dim3((unsigned)((n + 1023) / 1024), (unsigned)nlev);
+}
+// one block per (x-tile of 128, y) row of a single plane, for the boundary-plane kernels
+static inline dim3 rgrid(int ld, int ny) { return dim3((ld + 127) / 128, ny); }
+#define OBL_PLANE_LOOP(LD, NY)                                                                     \
+    for (int q_ = blockIdx.x * blockDim.x + threadIdx.x, n_ = (LD) * (NY); q_ < n_;               \
+         q_ += gridDim.x * blockDim.x)
 
 template <typename T>
 __global__ void k_vort(const T *__restrict__ u, const T *__restrict__ v, const T *__restrict__ dudy,
                        const T *__restrict__ dvdx, const T *__restrict__ dwdx, const T *__restrict__ dwdy,
                        T *o1, T *o2, T *o3, int nxt, int ldx, int nyt, int nz, T idz)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= ldx) return;
+    const int z = blockIdx.y;
+    OBL_PLANE_LOOP(ldx, nyt) {
+    const int x = q_ % ldx, y = q_ / ldx;
     const long long pl = (long long)ldx * nyt, o = (long long)y * ldx + x, c = o + pl * z;
     T r1 = 0, r2 = 0, r3 = 0;
     if (x < nxt && z >= 1) {
@@ -41,14 +54,15 @@ __global__ void k_vort(const T *__restrict__ u, const T *__restrict__ v, const T
     o1[c] = r1;
     o2[c] = r2;
     o3[c] = r3;
+    }
 }
 
 template <typename T>
 __global__ void k_cross(BigSet<T> b, T *X, T *Y, T *Z, int nx2, int ny2, int nz)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= nx2) return;
-    const long long P = (long long)nx2 * ny2, c = (long long)y * nx2 + x + P * z;
+    const int z = blockIdx.y;
+    OBL_PLANE_LOOP(nx2, ny2) {
+    const long long P = (long long)nx2 * ny2, c = q_ + P * z;
     const T h = (T)0.5;
     T rx = 0, ry = 0, rz = 0;
     if (z == 1) {
@@ -62,17 +76,21 @@ __global__ void k_cross(BigSet<T> b, T *X, T *Y, T *Z, int nx2, int ny2, int nz)
     X[c] = rx;
     Y[c] = ry;
     Z[c] = rz;
+    }
 }
 
 template <typename T>
 __global__ void k_update(T *u, T *v, T *w, const T *cx, const T *cy, const T *cz, T f, int nxt, int ldx, int nyt)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z + 1;
-    if (x >= nxt) return;
-    const long long c = (long long)y * ldx + x + (long long)ldx * nyt * z;
+    const int z = blockIdx.y + 1;
+    OBL_PLANE_LOOP(ldx, nyt) {
+    const int x = q_ % ldx;
+    if (x >= nxt) continue;
+    const long long c = q_ + (long long)ldx * nyt * z;
     u[c] -= f * cx[c];
     v[c] -= f * cy[c];
     w[c] -= f * cz[c];
+    }
 }
 
 template <typename T>
@@ -104,9 +122,9 @@ template <typename T>
 __global__ void k_cross_adj(BigSet<T> b, const T *__restrict__ LX, const T *__restrict__ LY,
                             const T *__restrict__ LZ, T f, CrossAdjOut<T> out, int nx2, int ny2, int nz)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= nx2) return;
-    const long long P = (long long)nx2 * ny2, o = (long long)y * nx2 + x, c = o + P * z;
+    const int z = blockIdx.y;
+    OBL_PLANE_LOOP(nx2, ny2) {
+    const long long P = (long long)nx2 * ny2, o = q_, c = o + P * z;
     // adjoints of X, Y at levels 1..nz-1 and of Z at 2..nz-1 (cross_z_big(1) is a constant)
     auto lx = [&](int k) -> T { return (k >= 1 && k <= nz - 1) ? f * LX[o + P * k] : (T)0; };
     auto ly = [&](int k) -> T { return (k >= 1 && k <= nz - 1) ? f * LY[o + P * k] : (T)0; };
@@ -131,14 +149,16 @@ __global__ void k_cross_adj(BigSet<T> b, const T *__restrict__ LX, const T *__re
     out.O1[c] = a1;
     out.O2[c] = a2;
     out.O3[c] = a3;
+    }
 }
 
 template <typename T>
 __global__ void k_adj_q(const T *s1, const T *s2, T *q1, T *q2, int nxt, int ldx, int nyt, int nz)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= ldx) return;
-    const long long pl = (long long)ldx * nyt, o = (long long)y * ldx + x, c = o + pl * z;
+    const int z = blockIdx.y;
+    OBL_PLANE_LOOP(ldx, nyt) {
+    const int x = q_ % ldx;
+    const long long pl = (long long)ldx * nyt, o = q_, c = o + pl * z;
     T r1 = 0, r2 = 0;
     if (x < nxt) {
         if (z >= 2 && z <= nz - 1) {
@@ -152,14 +172,17 @@ __global__ void k_adj_q(const T *s1, const T *s2, T *q1, T *q2, int nxt, int ldx
     }
     q1[c] = r1;
     q2[c] = r2;
+    }
 }
 
 template <typename T>
 __global__ void k_adj_combine(AdjCombineArgs<T> a, int nxt, int ldx, int nyt, int nz, T idz)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= nxt) return;
-    const long long pl = (long long)ldx * nyt, c = (long long)y * ldx + x + pl * z;
+    const int z = blockIdx.y;
+    OBL_PLANE_LOOP(ldx, nyt) {
+    const int x = q_ % ldx;
+    if (x >= nxt) continue;
+    const long long pl = (long long)ldx * nyt, c = q_ + pl * z;
     // transposed level difference of dudz(k) = (u(k) - u(k-1))/dz, k = 2..nz-1
     auto dzt = [&](const T *s) -> T {
         const T here = (z >= 2 && z <= nz - 1) ? s[c] : (T)0;
@@ -169,6 +192,7 @@ __global__ void k_adj_combine(AdjCombineArgs<T> a, int nxt, int ldx, int nyt, in
     a.lu[c] += a.sU[c] + a.t1[c] + dzt(a.s2);
     a.lv[c] += a.sV[c] - a.t2[c] - dzt(a.s1);
     a.lw[c] += a.sW[c] + a.t3[c] - a.t4[c];
+    }
 }
 
 constexpr int kKeThreads = 256;
@@ -223,7 +247,7 @@ void launch_vort(const T *u, const T *v, const T *dudy, const T *dvdx, const T *
                  T *o2, T *o3, int nxt, int ldx, int nyt, int nz, double dz, cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_vort<T><<<sgrid(ldx, nyt, nz + 1), 128, 0, s>>>(u, v, dudy, dvdx, dwdx, dwdy, o1, o2, o3, nxt, ldx, nyt,
+    k_vort<T><<<sgrid(ldx, nyt, nz + 1), 256, 0, s>>>(u, v, dudy, dvdx, dwdx, dwdy, o1, o2, o3, nxt, ldx, nyt,
                                                        nz, (T)(1.0 / dz));
     e = cudaGetLastError();
 }
@@ -232,7 +256,7 @@ void launch_cross(const BigSet<T> &b, T *X, T *Y, T *Z, int nx2, int ny2, int nz
                   cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_cross<T><<<sgrid(nx2, ny2, nz + 1), 128, 0, s>>>(b, X, Y, Z, nx2, ny2, nz);
+    k_cross<T><<<sgrid(nx2, ny2, nz + 1), 256, 0, s>>>(b, X, Y, Z, nx2, ny2, nz);
     e = cudaGetLastError();
 }
 template <typename T>
@@ -240,7 +264,7 @@ void launch_update(T *u, T *v, T *w, const T *cx, const T *cy, const T *cz, doub
                    int nyt, int nz, cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_update<T><<<sgrid(ldx, nyt, nz - 1), 128, 0, s>>>(u, v, w, cx, cy, cz, (T)f, nxt, ldx, nyt);
+    k_update<T><<<sgrid(ldx, nyt, nz - 1), 256, 0, s>>>(u, v, w, cx, cy, cz, (T)f, nxt, ldx, nyt);
     e = cudaGetLastError();
 }
 template <typename T>
@@ -248,14 +272,14 @@ void launch_adj_project_bc(T *lu, T *lv, T *lw, int ldx, int nyt, int nz, int st
                            cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_adj_project_bc<T><<<sgrid(ldx, nyt, 1), 128, 0, s>>>(lu, lv, lw, ldx, nyt, nz, stress_free);
+    k_adj_project_bc<T><<<rgrid(ldx, nyt), 128, 0, s>>>(lu, lv, lw, ldx, nyt, nz, stress_free);
     e = cudaGetLastError();
 }
 template <typename T>
 void launch_adj_w1(T *lw, const T *p, double c, int nxt, int ldx, int nyt, cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_adj_w1<T><<<sgrid(ldx, nyt, 1), 128, 0, s>>>(lw, p, (T)c, nxt, ldx, nyt);
+    k_adj_w1<T><<<rgrid(ldx, nyt), 128, 0, s>>>(lw, p, (T)c, nxt, ldx, nyt);
     e = cudaGetLastError();
 }
 template <typename T>
@@ -263,7 +287,7 @@ void launch_cross_adj(const BigSet<T> &b, const T *LX, const T *LY, const T *LZ,
                       const CrossAdjOut<T> &out, int nx2, int ny2, int nz, cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_cross_adj<T><<<sgrid(nx2, ny2, nz + 1), 128, 0, s>>>(b, LX, LY, LZ, (T)f, out, nx2, ny2, nz);
+    k_cross_adj<T><<<sgrid(nx2, ny2, nz + 1), 256, 0, s>>>(b, LX, LY, LZ, (T)f, out, nx2, ny2, nz);
     e = cudaGetLastError();
 }
 template <typename T>
@@ -271,7 +295,7 @@ void launch_adj_q(const T *s1, const T *s2, T *q1, T *q2, int nxt, int ldx, int 
                   cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_adj_q<T><<<sgrid(ldx, nyt, nz + 1), 128, 0, s>>>(s1, s2, q1, q2, nxt, ldx, nyt, nz);
+    k_adj_q<T><<<sgrid(ldx, nyt, nz + 1), 256, 0, s>>>(s1, s2, q1, q2, nxt, ldx, nyt, nz);
     e = cudaGetLastError();
 }
 template <typename T>
@@ -279,7 +303,7 @@ void launch_adj_combine(const AdjCombineArgs<T> &a, int nxt, int ldx, int nyt, i
                         cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    k_adj_combine<T><<<sgrid(nxt, nyt, nz + 1), 128, 0, s>>>(a, nxt, ldx, nyt, nz, (T)(1.0 / dz));
+    k_adj_combine<T><<<sgrid(ldx, nyt, nz + 1), 256, 0, s>>>(a, nxt, ldx, nyt, nz, (T)(1.0 / dz));
     e = cudaGetLastError();
 }
 template <typename T>
