@@ -79,3 +79,49 @@ def test_slab_split_matches_single_domain(prec, P, nx, ny, L):
             assert rel_l2(got["d"][i][:nx, :, lv], ref["d"][i][:nx, :, gl]) < tol, (r, "d", i)
         for i in range(4):
             assert rel_l2(got["big"][i][:, :, lv], ref["big"][i][:, :, gl]) < tol, (r, "big", i)
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+def test_slab_split_with_divtz_planes(prec):
+    """divtz(:,:,1) enters on the bottom rank and divtz(:,:,nz) on the top rank; the split
+    equals the single-domain step with the same planes."""
+    import torch
+    P, nx, ny, L = 2, 64, 64, 32
+    nzt = L + 1
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
+    rng = np.random.default_rng(5)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    planes = [torch.from_numpy(np.asarray(rng.standard_normal(((nx + 2) * ny,)))).to("cuda", dt)
+              for _ in range(2)]
+    P_ = lambda t: t.data_ptr()
+    one = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", **fields.DOMAIN)
+    b1 = Bufs(one, f)
+    io = b1.io()
+    one.step_dev(io.u, io.v, io.w, io.theta, list(io.d), list(io.big), io.p, list(io.dp),
+                 P_(planes[0]), P_(planes[1]))
+    one.synchronize()
+    ref = b1.get()
+    nzt_r, lz_r = slab.slab_grid(nx, ny, nzt, fields.DOMAIN["lz_tot"], P)
+    Lr = L // P
+    dom = dict(fields.DOMAIN, lz_tot=lz_r)
+    ctxs = [obl.Context(nx, ny, nzt_r, precision=prec, top_bc="neumann", **dom) for _ in range(P)]
+    bufs = [Bufs(c, {k: np.asfortranarray(v[:, :, r * Lr: r * Lr + Lr + 2]) for k, v in f.items()})
+            for r, c in enumerate(ctxs)]
+    ios = []
+    for r, b in enumerate(bufs):
+        x = b.io()
+        ios.append(obl.stepio_dev(x.u, x.v, x.w, x.theta, list(x.d), list(x.big), x.p, list(x.dp),
+                                  P_(planes[0]) if r == 0 else None, P_(planes[1]) if r == P - 1 else None))
+    steps = [slab.SlabStep(slab.LibBackend(c), r, P) for r, c in enumerate(ctxs)]
+    slab.step_lockstep(steps, ios)
+    torch.cuda.synchronize()
+    tol = 1e-11 if prec == "f64" else 2e-6
+    for r, b in enumerate(bufs):
+        got = b.get()
+        g0 = r * Lr
+        assert rel_l2(got["p"][:nx, :, 0: Lr + 1], ref["p"][:nx, :, g0: g0 + Lr + 1]) < tol, r
+        for i in range(3):
+            assert rel_l2(got["dp"][i][:nx, :, 0:Lr], ref["dp"][i][:nx, :, g0: g0 + Lr]) < tol, (r, i)
+        lv, gl = slice(1, Lr + 1), slice(g0 + 1, g0 + Lr + 1)
+        for k in ("u", "v", "w"):
+            assert rel_l2(got[k][:nx, :, lv], ref[k][:nx, :, gl]) < tol, (r, k)

@@ -88,3 +88,35 @@ def test_step_column_segments(orc, prec, nx, nzt):
     for segs in (0, 3, 16):
         assert rel_l2(outs[segs][0][:nx, :, : L + 1], outs[1][0][:nx, :, : L + 1]) < tol, segs
         assert rel_l2(outs[segs][1], outs[1][1]) < tol, segs
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("segs", [1, 0])
+def test_step_divtz_planes(orc, prec, segs):
+    """The step with divtz(:,:,1) and divtz(:,:,nz) planes (the boundary rows of the
+    pressure solve, 109_press_stag_array.f90:186-200) against the oracle's
+    press_stag_array + dpdz + project with the same planes; one sweep and column segments."""
+    nx, ny, nzt = 64, 48, 33
+    ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", **fields.DOMAIN)
+    ctx.set_param("tdma_segments", segs)
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
+    rng = np.random.default_rng(12)
+    pl = identical_inputs({k: np.asfortranarray(rng.standard_normal((g.ldx, ny))) for k in ("b", "t")}, prec)
+    u, v, w = (f[k].copy(order="F") for k in "uvw")
+    d, big, p, dp = _alloc_step(ctx)
+    ctx.step(u, v, w, f["theta"], d, big, p, dp, pl["b"], pl["t"])
+    rp, rdx, rdy = g.press_stag_array(f["u"], f["v"], f["w"], pl["b"], pl["t"], npz=2)
+    rdz = g.dpdz(rp)
+    ru, rv, rw = g.project(f["u"], f["v"], f["w"], rdx, rdy, rdz)
+    L = g.nz - 1
+    assert rel_l2(p[:nx, :, : L + 1], rp[:nx, :, : L + 1]) < TOL[prec]
+    for a, r in zip(dp, (rdx, rdy, rdz)):
+        assert rel_l2(a[:nx, :, :L], r[:nx, :, :L]) < TOL[prec]
+    for a, r in ((u, ru), (v, rv), (w, rw)):
+        assert rel_l2(a, r) < TOL[prec]
+    # the planes change the answer: the zero-plane step differs
+    u0, v0, w0 = (f[k].copy(order="F") for k in "uvw")
+    d0, big0, p0, dp0 = _alloc_step(ctx)
+    ctx.step(u0, v0, w0, f["theta"], d0, big0, p0, dp0)
+    assert rel_l2(p0[:nx, :, : L + 1], p[:nx, :, : L + 1]) > 1e-4
