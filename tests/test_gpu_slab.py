@@ -82,9 +82,11 @@ def test_slab_split_matches_single_domain(prec, P, nx, ny, L):
 
 
 @pytest.mark.parametrize("prec", ["f64", "mixed"])
-def test_slab_split_with_divtz_planes(prec):
-    """divtz(:,:,1) enters on the bottom rank and divtz(:,:,nz) on the top rank; the split
-    equals the single-domain step with the same planes."""
+@pytest.mark.parametrize("stress_free", [False, True])
+def test_slab_split_with_divtz_planes(prec, stress_free):
+    """divtz(:,:,1) enters on the bottom rank and divtz(:,:,nz) on the top rank, and the
+    stress-free copy of project() on the top rank only; the split equals the single-domain
+    step with the same planes and top condition."""
     import torch
     P, nx, ny, L = 2, 64, 64, 32
     nzt = L + 1
@@ -94,7 +96,8 @@ def test_slab_split_with_divtz_planes(prec):
     planes = [torch.from_numpy(np.asarray(rng.standard_normal(((nx + 2) * ny,)))).to("cuda", dt)
               for _ in range(2)]
     P_ = lambda t: t.data_ptr()
-    one = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", **fields.DOMAIN)
+    one = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", ubc_stress_free=stress_free,
+                      **fields.DOMAIN)
     b1 = Bufs(one, f)
     io = b1.io()
     one.step_dev(io.u, io.v, io.w, io.theta, list(io.d), list(io.big), io.p, list(io.dp),
@@ -104,7 +107,8 @@ def test_slab_split_with_divtz_planes(prec):
     nzt_r, lz_r = slab.slab_grid(nx, ny, nzt, fields.DOMAIN["lz_tot"], P)
     Lr = L // P
     dom = dict(fields.DOMAIN, lz_tot=lz_r)
-    ctxs = [obl.Context(nx, ny, nzt_r, precision=prec, top_bc="neumann", **dom) for _ in range(P)]
+    ctxs = [obl.Context(nx, ny, nzt_r, precision=prec, top_bc="neumann", ubc_stress_free=stress_free, **dom)
+            for _ in range(P)]
     bufs = [Bufs(c, {k: np.asfortranarray(v[:, :, r * Lr: r * Lr + Lr + 2]) for k, v in f.items()})
             for r, c in enumerate(ctxs)]
     ios = []

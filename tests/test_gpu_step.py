@@ -120,3 +120,22 @@ def test_step_divtz_planes(orc, prec, segs):
     d0, big0, p0, dp0 = _alloc_step(ctx)
     ctx.step(u0, v0, w0, f["theta"], d0, big0, p0, dp0)
     assert rel_l2(p0[:nx, :, : L + 1], p[:nx, :, : L + 1]) > 1e-4
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+def test_step_stress_free_top(orc, prec):
+    """ubc_mom = 'stress free': project copies u, v of level nz-2 into nz-1
+    (110_project.f90:50-60) in the fused step, against the oracle's step."""
+    nx, ny, nzt = 64, 64, 33
+    ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", ubc_stress_free=True, **fields.DOMAIN)
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN, ubc_stress_free=True)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
+    u, v, w = (f[k].copy(order="F") for k in "uvw")
+    d, big, p, dp = _alloc_step(ctx)
+    ctx.step(u, v, w, f["theta"], d, big, p, dp)
+    ref = g.step(f["u"], f["v"], f["w"], f["theta"], npz=2)
+    for a, k in ((u, "u"), (v, "v"), (w, "w")):
+        assert rel_l2(a, ref[k]) < TOL[prec], k
+    nz = g.nz
+    assert np.array_equal(u[:nx, :, nz - 1], u[:nx, :, nz - 2])
+    assert np.array_equal(v[:nx, :, nz - 1], v[:nx, :, nz - 2])
