@@ -29,16 +29,17 @@ __global__ void __launch_bounds__(32 * NW, TWG ? 4 : 1) k_cols_divt(ColArgs<T> a
 template <typename T, int N>
 static cudaError_t launch_divt_n(const ColArgs<T> &a, const DivEpi<T> &e, cudaStream_t s)
 {
-    static bool init = false;
+    static bool inits[kMaxDevices] = {};
     constexpr int NW = col_warps<T, N, OP_DERIV>(), WB = col_lines<T, N, OP_DERIV>();
     constexpr bool TWG = col_tw_global<T, N, OP_DERIV>();
     using D = LineDerived<N, OP_DERIV>;
     const size_t sm = TWG ? sizeof(C2<T>) * (size_t)D::NM * WB : cols2_smem<T, N, OP_DERIV, WB>();
     auto kern = k_cols_divt<T, N, NW, WB, TWG>;
-    if (!init) {
+    const int ds = device_slot();
+    if (ds < 0 || !inits[ds]) {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (err != cudaSuccess) return err;
-        init = true;
+        if (ds >= 0) inits[ds] = true;
     }
     const int nlines = a.ncols / 2;
     dim3 grid((nlines + WB - 1) / WB, a.nlev);

@@ -227,11 +227,12 @@ __global__ void __launch_bounds__(256, MINB) k_ensemble(EnsArgs<T> e)
 
 template <typename T, int PB, int PE, int MINB> cudaError_t EnsKernel<T, PB, PE, MINB>::attr(size_t smem)
 {
-    static size_t set = 0;
-    if (smem <= set) return cudaSuccess;
+    static size_t sets[kMaxDevices] = {};
+    const int ds = device_slot();
+    if (ds >= 0 && smem <= sets[ds]) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(k_ensemble<T, PB, PE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
-    if (e == cudaSuccess) set = smem;
+    if (e == cudaSuccess && ds >= 0) sets[ds] = smem;
     return e;
 }
 

@@ -14,6 +14,17 @@
 
 namespace obl {
 
+// Kernel launchers cache one-time set-up (function attributes, occupancy-derived grid
+// caps).  Both belong to a device context, so the caches are kept per device; past
+// kMaxDevices the set-up is redone on every launch.
+constexpr int kMaxDevices = 64;
+inline int device_slot()
+{
+    int d = 0;
+    cudaGetDevice(&d);
+    return (d >= 0 && d < kMaxDevices) ? d : -1;
+}
+
 // ----------------------------------------------------------------------------- complex
 template <typename T> struct cplx_t;
 template <> struct cplx_t<float> { using type = float2; };

@@ -23,18 +23,19 @@ template <typename T, int N> static cudaLaunchConfig_t fwd_cfg(int ncl, int csiz
 
 template <typename T, int N> static cudaError_t fwd_prepare(int csize)
 {
-    static bool init = false, big = false;
+    static bool inits[kMaxDevices] = {}, bigs[kMaxDevices] = {};
     auto kern = k_fwd_fused<T, N>;
-    if (!init) {
+    const int ds = device_slot();
+    if (ds < 0 || !inits[ds]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)FwdFusedGeo<T, N>::smem);
         if (e != cudaSuccess) return e;
-        init = true;
+        if (ds >= 0) inits[ds] = true;
     }
-    if (csize > 8 && !big) {
+    if (csize > 8 && (ds < 0 || !bigs[ds])) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
-        big = true;
+        if (ds >= 0) bigs[ds] = true;
     }
     return cudaSuccess;
 }
@@ -105,8 +106,10 @@ template <typename T, int N> static cudaError_t rows3_run_n(const RowsFwd3Args<T
 {
     using GG = FwdFusedGeo<T, N>;
     const size_t sm = sizeof(C2<T>) * ((size_t)GG::TF + GG::TB + GG::TPB) + GG::row_scr;
-    static int cap = 0;
+    static int caps[kMaxDevices] = {};
     auto kern = k_rows_fwd3<T, N>;
+    const int ds = device_slot();
+    int cap = ds >= 0 ? caps[ds] : 0;
     if (!cap) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
@@ -115,6 +118,7 @@ template <typename T, int N> static cudaError_t rows3_run_n(const RowsFwd3Args<T
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
         cap = nsm * (per > 0 ? per : 1);
+        if (ds >= 0) caps[ds] = cap;
     }
     const long long per_cta = 8LL * GG::LPW;
     const long long want = (a.npairs + per_cta - 1) / per_cta;
@@ -145,12 +149,13 @@ template <typename T, int N> static cudaError_t pinv_cols_n(const PinvColArgs<T>
     constexpr bool TWG = false;
     constexpr int NW = TWG ? 8 : col_warps<T, N, OP_INV>();
     const size_t sm = sizeof(C2<T>) * ((TWG ? 0 : (size_t)D::TB) + (size_t)N * LmGeo<T>::WB);
-    static bool init = false;
+    static bool inits[kMaxDevices] = {};
     auto kern = k_cols_pinv<T, N, NW, TWG>;
-    if (!init) {
+    const int ds = device_slot();
+    if (ds < 0 || !inits[ds]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        init = true;
+        if (ds >= 0) inits[ds] = true;
     }
     dim3 grid((a.lhx + LmGeo<T>::WB - 1) / LmGeo<T>::WB, nlev);
     kern<<<grid, 32 * NW, sm, s>>>(a);
@@ -161,8 +166,10 @@ template <typename T, int N> static cudaError_t pinv_rows_n(const PinvRowArgs<T>
 {
     using D = LineDerived<N, OP_INV>;
     const size_t sm = sizeof(C2<T>) * ((size_t)D::TB + (size_t)8 * D::LPW * scratch_len(N));
-    static int cap = 0;
+    static int caps[kMaxDevices] = {};
     auto kern = k_rows_pinv<T, N>;
+    const int ds = device_slot();
+    int cap = ds >= 0 ? caps[ds] : 0;
     if (!cap) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
@@ -171,6 +178,7 @@ template <typename T, int N> static cudaError_t pinv_rows_n(const PinvRowArgs<T>
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
         cap = nsm * (per > 0 ? per : 1);
+        if (ds >= 0) caps[ds] = cap;
     }
     const long long items = 4 * ((a.npairs + D::LPW - 1) / D::LPW);   // (pair group, component)
     const long long want = (items + 7) / 8;

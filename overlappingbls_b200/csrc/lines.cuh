@@ -764,9 +764,11 @@ template <typename T, int N, int OP, bool REAL> inline size_t cols_smem()
 
 template <typename T, int N, int OP> cudaError_t launch_rows_t(const RowArgs<T> &a, cudaStream_t s)
 {
-    static int grid_cap = 0;
+    static int caps[kMaxDevices] = {};
     const size_t sm = rows_smem<T, N, OP>();
     auto kern = k_rows<T, N, OP>;
+    const int ds = device_slot();
+    int grid_cap = ds >= 0 ? caps[ds] : 0;
     if (!grid_cap) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
@@ -775,6 +777,7 @@ template <typename T, int N, int OP> cudaError_t launch_rows_t(const RowArgs<T> 
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, sm);
         grid_cap = nsm * (per > 0 ? per : 1);
+        if (ds >= 0) caps[ds] = grid_cap;
     }
     constexpr int LPW = LineDerived<N, OP>::LPW;
     const long long per_cta = 8LL * LPW;
@@ -793,14 +796,15 @@ template <typename T, int N, int OP, int WB = LmGeo<T>::WB> inline size_t cols2_
 
 template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const ColArgs<T> &a0, cudaStream_t s)
 {
-    static bool init = false;
-    static int resident = 0;   // CTAs of this kernel resident on the whole GPU
+    static int residents[kMaxDevices] = {};   // CTAs of this kernel resident on the whole GPU
     constexpr int NW = col_warps<T, N, OP>(), WB = col_lines<T, N, OP>();
     constexpr bool TWG = col_tw_global<T, N, OP>();
     using D = LineDerived<N, OP>;
     const size_t sm = TWG ? sizeof(C2<T>) * (size_t)D::NM * WB : cols2_smem<T, N, OP, WB>();
     auto kern = k_cols2<T, N, OP, REAL, NW, WB, TWG>;
-    if (!init) {
+    const int ds = device_slot();
+    int resident = ds >= 0 ? residents[ds] : 0;
+    if (!resident) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         int dev = 0, nsm = 0, per = 0;
@@ -808,7 +812,7 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * NW, sm);
         resident = nsm * (per > 0 ? per : 1);
-        init = true;
+        if (ds >= 0) residents[ds] = resident;
     }
     ColArgs<T> a = a0;
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
