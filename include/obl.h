@@ -333,6 +333,12 @@ int obl_ensemble_time_dev(obl_ensemble *ens, const obl_step_io *ios, int use_gra
 int obl_ensemble_phase_times(obl_ensemble *ens, int on, double *ms, int n);
 int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n);
 
+/* Failure-path self-test (no counterpart in the reference): one CTA runs the persistent
+   kernel's grid barrier on the context's stream.  never_released = 0: the barrier
+   releases, OBL_OK.  never_released = 1: no other CTA ever arrives, the bounded wait gives
+   up after a few seconds and OBL_ERR_TIMEOUT is returned, the context staying usable. */
+int obl_selftest_grid_barrier(obl_ctx *ctx, int never_released);
+
 /* ---- the step on a z-slab of a domain split over nranks ranks (one GPU each) ----
    The reference splits z over npz MPI ranks and pipelines its Thomas sweeps rank by rank
    with a send/recv per y-row (109_press_stag_array.f90:244-319, 103_flosol.f90:169-173).

@@ -40,7 +40,7 @@ EXPORTS = [
     "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
     "obl_divstress_uv", "obl_divstress_w", "obl_divstress_uv_dev", "obl_divstress_w_dev",
     "obl_write_file_3d_dev", "obl_read_file_3d_dev", "obl_checkpoint_final_dev", "obl_read_flow_field_dev",
-    "obl_read_total_time", "obl_write_total_time",
+    "obl_read_total_time", "obl_write_total_time", "obl_selftest_grid_barrier",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
     "obl_zero_padding", "obl_zero_unpadding", "obl_zero_padding_dev", "obl_zero_unpadding_dev",
     "obl_zero_padding_noalloc_dev",
@@ -129,6 +129,7 @@ def load_library(path=LIB_PATH):
         "obl_read_flow_field_dev": [ctx, ctypes.c_char_p, I, ctypes.POINTER(P), I, I],
         "obl_read_total_time": [ctypes.c_char_p, ctypes.POINTER(I)],
         "obl_write_total_time": [ctypes.c_char_p, I],
+        "obl_selftest_grid_barrier": [ctx, I],
         "obl_fftn": [ctx, P, P, I], "obl_ifftn": [ctx, P, P, I],
         "obl_fftn_dev": [ctx, P, P, I], "obl_ifftn_dev": [ctx, P, P, I],
         "obl_zero_padding": [ctx, P, P, I], "obl_zero_unpadding": [ctx, P, P, I],
@@ -385,6 +386,12 @@ class Context:
 
     def ddz_w_dev(self, dfdz, fun):
         self._check(self._lib.obl_ddz_w_dev(self._h, dfdz, fun), "ddz_w_dev")
+
+    def selftest_grid_barrier(self, never_released=False):
+        """The persistent ensemble kernel's grid barrier in one CTA: returns when it
+        releases; raises OblError (OBL_ERR_TIMEOUT) when its bounded wait gives up."""
+        self._check(self._lib.obl_selftest_grid_barrier(self._h, 1 if never_released else 0),
+                    "selftest_grid_barrier")
 
     # ---- restart files (integer device pointers; FP64 files, see include/obl.h) ----
     def write_file_3d_dev(self, var, fn, disp0=0, zrank=0, nzranks=1):

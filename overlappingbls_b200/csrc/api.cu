@@ -1498,6 +1498,14 @@ int obl_ddz_uv_dev(obl_ctx *ctx, void *dfdz, const void *fun)
     if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
     DEVCALL(ctx, return o.ddz_uv((T *)dfdz, (const T *)fun););
 }
+int obl_selftest_grid_barrier(obl_ctx *ctx, int never_released)
+{
+    if (!ctx) return OBL_ERR_ARG;
+    if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice");
+    std::string err;
+    const int rc = ens_barrier_selftest(never_released != 0, ctx->stream, err);
+    return rc ? fail(ctx, rc, err) : OBL_OK;
+}
 int obl_divstress_uv_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz)
 {
     if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2) return OBL_ERR_ARG;

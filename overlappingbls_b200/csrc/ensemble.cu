@@ -3,6 +3,7 @@
 #include <algorithm>
 
 #include "ensemble_kernel.cuh"
+#include "obl.h"
 
 namespace obl {
 
@@ -17,6 +18,45 @@ bool ens_length_supported(int n)
 }
 
 template <typename T> int ens_wb() { return LmGeo<T>::WB; }
+
+// ----------------------------------------------------------------------------- self-test
+// One CTA through the grid barrier with its arrival counter preset: 0 releases at once;
+// any other value never reaches the release count (nothing else arrives), so the bounded
+// wait gives up and raises the error flag, as a lost CTA of a real launch would.
+__global__ void k_barrier_selftest(unsigned *bar, int *passed)
+{
+    const bool ok = ens_barrier(bar, reinterpret_cast<int *>(bar + 2));
+    if (threadIdx.x == 0) *passed = ok ? 1 : 0;
+}
+
+int ens_barrier_selftest(bool never_released, cudaStream_t s, std::string &err)
+{
+    unsigned *bar = nullptr;   // arrivals, generation, error flag, passed
+    if (cudaMalloc(&bar, 4 * sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        err = "barrier self-test: allocation failed";
+        return OBL_ERR_NOMEM;
+    }
+    const unsigned init[4] = {never_released ? 1u : 0u, 0u, 0u, 0u};
+    cudaError_t e = cudaMemcpyAsync(bar, init, sizeof init, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        k_barrier_selftest<<<1, 128, 0, s>>>(bar, reinterpret_cast<int *>(bar + 3));
+        e = cudaGetLastError();
+    }
+    unsigned out[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, bar, sizeof out, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(bar);
+    if (e != cudaSuccess) {
+        err = std::string("barrier self-test: ") + cudaGetErrorString(e);
+        return OBL_ERR_CUDA;
+    }
+    if (out[2]) {
+        err = "barrier self-test: the grid-barrier wait gave up";
+        return OBL_ERR_TIMEOUT;
+    }
+    return out[3] ? OBL_OK : OBL_ERR_TIMEOUT;
+}
 
 // ----------------------------------------------------------------------------- host side
 template <typename T> long long EnsGeoHost<T>::rows_units(int n, long long npairs)

@@ -11,6 +11,8 @@
 // and every unit dispatches at run time on its instance's line lengths to the same
 // device functions the single-instance kernels use.
 #pragma once
+#include <string>
+
 #include "fused.cuh"
 #include "press.cuh"
 
@@ -55,6 +57,9 @@ template <typename T> struct EnsArgs {
 
 // host-side geometry of the instance kernels (per line length n; 0 if unsupported)
 bool ens_length_supported(int n);
+// The persistent kernel's grid barrier run by one CTA: OBL_OK when it releases,
+// OBL_ERR_TIMEOUT when (never_released) its bounded wait gives up.
+int ens_barrier_selftest(bool never_released, cudaStream_t s, std::string &err);
 template <typename T> struct EnsGeoHost {
     static long long rows_units(int n, long long npairs);      // units of the row pass
     static long long pinv_rows_units(int n, long long npairs); // units of the x-inverse

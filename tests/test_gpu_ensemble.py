@@ -193,3 +193,24 @@ def test_autotune_ensemble_and_step(tmp_path):
     assert t is not None and p in tune.step_candidates(ctx.nxt, ctx.nyt)
     print("autotune:", best, ms, "step", p, t)
     ens.close()
+
+
+def test_grid_barrier_wait_gives_up():
+    """The persistent kernel's grid barrier, run by one CTA: it releases when it should;
+    with no other CTA ever arriving, its bounded wait gives up, the host reads
+    OBL_ERR_TIMEOUT, and the context keeps working."""
+    import time
+    ctx = obl.Context(32, 32, 9, precision="mixed", **fields.DOMAIN)
+    ctx.selftest_grid_barrier(False)
+    t0 = time.perf_counter()
+    with pytest.raises(obl.OblError, match="OBL_ERR_TIMEOUT"):
+        ctx.selftest_grid_barrier(True)
+    waited = time.perf_counter() - t0
+    assert waited < 60.0
+    ctx.selftest_grid_barrier(False)
+    f = fields.make_fields(32, 32, 9)
+    out = ctx.field()
+    ctx.ddx(out, f["u"])
+    assert np.isfinite(out[:32]).all()
+    print(f"grid barrier: the never-released wait gave up after {waited:.1f} s")
+    ctx.close()
