@@ -139,3 +139,49 @@ def test_step_stress_free_top(orc, prec):
     nz = g.nz
     assert np.array_equal(u[:nx, :, nz - 1], u[:nx, :, nz - 2])
     assert np.array_equal(v[:nx, :, nz - 1], v[:nx, :, nz - 2])
+
+
+@pytest.mark.parametrize("prec", ["mixed", "f64"])
+def test_headline_size_step_is_divergence_free(prec):
+    """512x512 with 256 levels (the headline workload), a size-independent property: after
+    the step's projection (Neumann top, band-limited u, v, w with w = 0 at levels 1 and
+    nz) the discrete divergence ddx(u) + ddy(v) + (w(k+1) - w(k))/dz vanishes at every
+    level 1..nz-1, as the pressure equation's right-hand side defines it."""
+    import torch
+    nx = ny = 512
+    nzt = 257
+    ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", **fields.DOMAIN)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    ldx, nz = ctx.ldx, ctx.nz
+    dev = "cuda"
+    X = (torch.arange(ldx, device=dev, dtype=torch.float64) * (2 * np.pi / nx))[None, None, :]
+    Y = (torch.arange(ny, device=dev, dtype=torch.float64) * (2 * np.pi / ny))[None, :, None]
+    k = torch.arange(nz + 1, device=dev, dtype=torch.float64)[:, None, None]
+    hz = torch.where(k >= 1, torch.sin(np.pi * (k - 1) / (nz - 1)), torch.zeros_like(k))
+    gen = torch.Generator(device="cpu").manual_seed(7)
+    amp = torch.randn(3, 6, generator=gen, dtype=torch.float64).tolist()
+    u = sum(a * torch.sin(m * X + 0.3 * m) * torch.cos((m + 1) * Y) for m, a in zip(range(1, 7), amp[0])) * (1 + 0.01 * k)
+    v = sum(a * torch.cos((m + 2) * X) * torch.sin(m * Y + 0.1) for m, a in zip(range(1, 7), amp[1])) * (2 - 0.004 * k)
+    w = sum(a * torch.sin(m * X) * torch.sin((m + 3) * Y) for m, a in zip(range(1, 7), amp[2])) * hz
+    th = 300.0 + 0.01 * k + 0.0 * X + 0.0 * Y
+    S = {n: t.to(dt).contiguous().reshape(-1) for n, t in (("u", u), ("v", v), ("w", w), ("t", th))}
+    del u, v, w, th
+    nf, nd, nb = ldx * ny * (nz + 1), ldx * ny * nz, ctx.nxt2 * ctx.nyt2 * (nz + 1)
+    d = [torch.empty(nf, dtype=dt, device=dev) for _ in range(8)]
+    big = [torch.empty(nb, dtype=dt, device=dev) for _ in range(4)]
+    p = torch.empty(nf, dtype=dt, device=dev)
+    dp = [torch.empty(nd, dtype=dt, device=dev) for _ in range(3)]
+    P = lambda t: t.data_ptr()
+    ctx.step_dev(P(S["u"]), P(S["v"]), P(S["w"]), P(S["t"]), [P(t) for t in d], [P(t) for t in big], P(p),
+                 [P(t) for t in dp])
+    dudx, dvdy = torch.empty_like(p), torch.empty_like(p)
+    ctx.ddx_dev(P(dudx), P(S["u"]), nz + 1)
+    ctx.ddy_dev(P(dvdy), P(S["v"]), nz + 1)
+    ctx.synchronize()
+    shp = (nz + 1, ny, ldx)
+    a, b, W = dudx.view(shp).double(), dvdy.view(shp).double(), S["w"].view(shp).double()
+    div = a[1:nz, :, :nx] + b[1:nz, :, :nx] + (W[2:nz + 1, :, :nx] - W[1:nz, :, :nx]) / ctx.info["dz"]
+    rel = float(div.abs().max() / a[1:nz, :, :nx].abs().max())
+    print(f"headline-size step ({prec}): max |div| / max |ddx(u)| = {rel:.2e}")
+    assert rel < (1e-11 if prec == "f64" else 2e-4)
+    ctx.close()
