@@ -239,6 +239,84 @@ template <typename T> struct Ops {
         return cols(OP_UNPAD, true, ny, ca, "unpad_cols");
     }
 
+    // ---- several fields of one shape per launch (the rollout's convec and its transpose:
+    // small grids whose single-field launches do not fill the GPU) ----
+    int rows_multi(int op, int n, const RowArgs<T> &a, const MultiPtr<T> &m, int nf, const char *name)
+    {
+        LaunchScope ls(ctx->rec, name, s());
+        return chk(launch_rows_multi<T>(op, n, a, m, nf, s()), name);
+    }
+    int cols_multi(int op, int n, const ColArgs<T> &a, const MultiPtr<T> &m, int nf, const char *name)
+    {
+        LaunchScope ls(ctx->rec, name, s());
+        return chk(launch_cols_multi<T>(op, n, a, m, nf, s()), name);
+    }
+    int pad_multi(const T *const *src, T *const *big, int nf, int nlev)
+    {
+        const int nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        const size_t xsz = (size_t)nx2 * ny * nlev;
+        int rc = ensure(ctx, ctx->tmp, sizeof(T) * xsz * nf);
+        if (rc) return rc;
+        T *xb = (T *)ctx->tmp.p;
+        MultiPtr<T> mr{}, mc{};
+        for (int f = 0; f < nf; ++f) {
+            mr.src[f] = src[f];
+            mr.dst[f] = xb + f * xsz;
+            mc.src[f] = xb + f * xsz;
+            mc.dst[f] = big[f];
+        }
+        auto ra = rowargs(nullptr, ctx->ldx, nullptr, nx2, (long long)ny * nlev, 1.0 / nx, OP_PAD, nx);
+        if ((rc = rows_multi(OP_PAD, nx, ra, mr, nf, "pad_rows"))) return rc;
+        auto ca = colargs(nullptr, nx2, (long long)nx2 * ny, nullptr, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny,
+                          OP_PAD, ny);
+        return cols_multi(OP_PAD, ny, ca, mc, nf, "pad_cols");
+    }
+    int unpad_multi(const T *const *big, T *const *var, int nf, int nlev)
+    {
+        const int nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
+        const size_t xsz = (size_t)nx * ny2 * nlev;
+        int rc = ensure(ctx, ctx->tmp, sizeof(T) * xsz * nf);
+        if (rc) return rc;
+        T *xs = (T *)ctx->tmp.p;
+        MultiPtr<T> mr{}, mc{};
+        for (int f = 0; f < nf; ++f) {
+            mr.src[f] = big[f];
+            mr.dst[f] = xs + f * xsz;
+            mc.src[f] = xs + f * xsz;
+            mc.dst[f] = var[f];
+        }
+        auto ra = rowargs(nullptr, nx2, nullptr, nx, (long long)ny2 * nlev, 1.0 / nx2, OP_UNPAD, nx);
+        if ((rc = rows_multi(OP_UNPAD, nx, ra, mr, nf, "unpad_rows"))) return rc;
+        auto ca = colargs(nullptr, nx, (long long)nx * ny2, nullptr, ctx->ldx, ctx->plane(), nx, nlev, 1.0 / ny2,
+                          OP_UNPAD, ny);
+        ca.pad_copy = 1;
+        return cols_multi(OP_UNPAD, ny, ca, mc, nf, "unpad_cols");
+    }
+    int ddx_multi(T *const *out, const T *const *in, int nf, int nlev)
+    {
+        MultiPtr<T> m{};
+        for (int f = 0; f < nf; ++f) {
+            m.src[f] = in[f];
+            m.dst[f] = out[f];
+        }
+        auto a = rowargs(nullptr, ctx->ldx, nullptr, ctx->ldx, (long long)ctx->nyt * nlev, 1.0 / ctx->nxt, OP_DERIV,
+                         ctx->nxt);
+        a.ktab = ctx->d_kx;
+        return rows_multi(OP_DERIV, ctx->nxt, a, m, nf, "ddx_rows");
+    }
+    int ddy_multi(T *const *out, const T *const *in, int nf, int nlev)
+    {
+        MultiPtr<T> m{};
+        for (int f = 0; f < nf; ++f) {
+            m.src[f] = in[f];
+            m.dst[f] = out[f];
+        }
+        auto a = colargs(nullptr, ctx->ldx, ctx->plane(), nullptr, ctx->ldx, ctx->plane(), ctx->nxt, nlev,
+                         1.0 / ctx->nyt, OP_DERIV, ctx->nyt);
+        a.ktab = ctx->d_ky1;
+        return cols_multi(OP_DERIV, ctx->nyt, a, m, nf, "ddy_cols");
+    }
+
     // ---- fftn / ifftn (203_fftn_mpi.f90:4-67) ----
     // real planes (ldx stride) -> complex planes (lhx stride), nlev planes
     int fftn(const T *in, C2<T> *out, int nlev, double scale)
@@ -658,9 +736,11 @@ template <typename T> struct Ops {
     {
         const int nlev = ctx->nz + 1;
         int rc;
-        if ((rc = ddy(rs(S_DUDY), u, nlev)) || (rc = ddx(rs(S_DVDX), v, nlev)) || (rc = ddx(rs(S_DWDX), w, nlev)) ||
-            (rc = ddy(rs(S_DWDY), w, nlev)))
-            return rc;
+        {
+            const T *xin[2] = {v, w}, *yin[2] = {u, w};
+            T *xout[2] = {rs(S_DVDX), rs(S_DWDX)}, *yout[2] = {rs(S_DUDY), rs(S_DWDY)};
+            if ((rc = ddx_multi(xout, xin, 2, nlev)) || (rc = ddy_multi(yout, yin, 2, nlev))) return rc;
+        }
         {
             cudaError_t e = cudaSuccess;
             LaunchScope ls(ctx->rec, "vort", s());
@@ -669,9 +749,8 @@ template <typename T> struct Ops {
             if ((rc = chk(e, "vort"))) return rc;
         }
         const T *src[6] = {u, v, w, rs(S_O1), rs(S_O2), rs(S_O3)};
-        for (int i = 0; i < 6; ++i)
-            if ((rc = pad(src[i], rb(B_U + i), nlev))) return rc;
-        return OBL_OK;
+        T *big[6] = {rb(B_U), rb(B_V), rb(B_W), rb(B_O1), rb(B_O2), rb(B_O3)};
+        return pad_multi(src, big, 6, nlev);
     }
 
     // convec (108_convec.f90:11-99): cx, cy, cz at levels 1..nz-1
@@ -686,10 +765,9 @@ template <typename T> struct Ops {
             if ((rc = chk(e, "cross"))) return rc;
         }
         const long long pl = ctx->plane(), plb = (long long)ctx->nxt2 * ctx->nyt2;
-        T *dst[3] = {cx, cy, cz};
-        for (int i = 0; i < 3; ++i)
-            if ((rc = unpad(rb(B_X + i) + plb, dst[i] + pl, ctx->nz - 1))) return rc;
-        return OBL_OK;
+        const T *src[3] = {rb(B_X) + plb, rb(B_Y) + plb, rb(B_Z) + plb};
+        T *dst[3] = {cx + pl, cy + pl, cz + pl};
+        return unpad_multi(src, dst, 3, ctx->nz - 1);
     }
 
     // P: press_stag_array (divtz = 0) + dpdz + project, in place
@@ -749,9 +827,11 @@ template <typename T> struct Ops {
         // adjoints of cx, cy, cz: pad(lambda) scaled by -dt*tadv1 inside the transposed
         // cross product (unpad^T = pad/2.25 and pad^T = 2.25*unpad cancel)
         if ((rc = convec_fields(u, v, w))) return rc;
-        T *lam[3] = {lu, lv, lw};
-        for (int i = 0; i < 3; ++i)
-            if ((rc = pad(lam[i], rb(B_X + i), nlev))) return rc;
+        {
+            const T *lam[3] = {lu, lv, lw};
+            T *big[3] = {rb(B_X), rb(B_Y), rb(B_Z)};
+            if ((rc = pad_multi(lam, big, 3, nlev))) return rc;
+        }
         {
             cudaError_t e = cudaSuccess;
             LaunchScope ls(ctx->rec, "cross_adj", s());
@@ -761,8 +841,11 @@ template <typename T> struct Ops {
             if ((rc = chk(e, "cross_adj"))) return rc;
         }
         // sU, sV, sW, s1, s2, s3 (unpadded adjoints) into the first six small fields
-        for (int i = 0; i < 6; ++i)
-            if ((rc = unpad(rb(B_AU + i), rs(S_DUDY + i), nlev))) return rc;
+        {
+            const T *src[6] = {rb(B_AU), rb(B_AV), rb(B_AW), rb(B_A1), rb(B_A2), rb(B_A3)};
+            T *dst[6] = {rs(S_DUDY), rs(S_DVDX), rs(S_DWDX), rs(S_DWDY), rs(S_O1), rs(S_O2)};
+            if ((rc = unpad_multi(src, dst, 6, nlev))) return rc;
+        }
         T *sU = rs(S_DUDY), *sV = rs(S_DVDX), *sW = rs(S_DWDX), *s1 = rs(S_DWDY), *s2 = rs(S_O1), *s3 = rs(S_O2);
         T *q1 = rs(S_O3), *q2 = rs(S_CX);
         {
@@ -772,9 +855,11 @@ template <typename T> struct Ops {
             if ((rc = chk(e, "adj_q"))) return rc;
         }
         // ddx^T = -ddx, ddy^T = -ddy: the signs are applied in the combine kernel
-        if ((rc = ddy(rs(S_T1), s3, nlev)) || (rc = ddx(rs(S_T2), s3, nlev)) || (rc = ddx(rs(S_T3), q2, nlev)) ||
-            (rc = ddy(rs(S_T4), q1, nlev)))
-            return rc;
+        {
+            const T *xin[2] = {s3, q2}, *yin[2] = {s3, q1};
+            T *xout[2] = {rs(S_T2), rs(S_T3)}, *yout[2] = {rs(S_T1), rs(S_T4)};
+            if ((rc = ddx_multi(xout, xin, 2, nlev)) || (rc = ddy_multi(yout, yin, 2, nlev))) return rc;
+        }
         cudaError_t e = cudaSuccess;
         LaunchScope ls(ctx->rec, "adj_combine", s());
         AdjCombineArgs<T> a{lu, lv, lw, sU, sV, sW, s1, s2, rs(S_T1), rs(S_T2), rs(S_T3), rs(S_T4)};

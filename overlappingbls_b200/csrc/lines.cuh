@@ -827,6 +827,19 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
 // Runtime dispatch: n is the base length (the unpadded one for PAD/UNPAD).
 template <typename T> cudaError_t launch_rows(int op, int n, const RowArgs<T> &a, cudaStream_t s);
 template <typename T> cudaError_t launch_cols(int op, bool real, int n, const ColArgs<T> &a, cudaStream_t s);
+
+// The same real-line ops (OP_DERIV, OP_PAD, OP_UNPAD) on up to kMultiFields fields of
+// one shape in one launch: field f reads src[f] and writes dst[f]; the args' src/dst are
+// ignored.  For grids whose single-field launches are too small to fill the GPU.
+constexpr int kMultiFields = 6;
+template <typename T> struct MultiPtr {
+    const void *src[kMultiFields];
+    void *dst[kMultiFields];
+};
+template <typename T>
+cudaError_t launch_rows_multi(int op, int n, const RowArgs<T> &a, const MultiPtr<T> &m, int nf, cudaStream_t s);
+template <typename T>
+cudaError_t launch_cols_multi(int op, int n, const ColArgs<T> &a, const MultiPtr<T> &m, int nf, cudaStream_t s);
 bool line_length_supported(int n);
 // twiddle table (interleaved re,im in FP64) of the plan with the given role for base length n
 std::vector<double> plan_table(int n, int role);
