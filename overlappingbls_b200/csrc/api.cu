@@ -379,12 +379,13 @@ template <typename T> struct Ops {
         const double cst = 1.0 / ((double)nx * ny);               // :153
         const double sc = (cst / kTadv1) * (1.0 / ctx->dt_nd);     // rH = const/tadv1*(u/dt) (:166-168)
 
-        // x r2c of levels 1..L of u, v, w straight into the spectral buffers
-        const T *src[3] = {u, v, w};
-        C2<T> *dst[3] = {Hx, Hy, Hz};
-        for (int c = 0; c < 3 && !rhs_ready; ++c) {
-            auto ra = rowargs(src[c] + pl, ldx, dst[c] + S, lhx, (long long)ny * L, sc, OP_FWD, nx);
-            if ((rc = rows(OP_FWD, nx, ra, "press_fwd_rows"))) return rc;
+        // x r2c of levels 1..L of u, v, w straight into the spectral buffers (one launch)
+        if (!rhs_ready) {
+            MultiPtr<T> m{};
+            m.src[0] = u + pl; m.src[1] = v + pl; m.src[2] = w + pl;
+            m.dst[0] = Hx + S; m.dst[1] = Hy + S; m.dst[2] = Hz + S;
+            auto ra = rowargs(nullptr, ldx, nullptr, lhx, (long long)ny * L, sc, OP_FWD, nx);
+            if ((rc = rows_multi(OP_FWD, nx, ra, m, 3, "press_fwd_rows"))) return rc;
         }
         // boundary planes H_z(0) and H_z(nz) (:186-200)
         if (dbot) {
@@ -401,11 +402,13 @@ template <typename T> struct Ops {
         }
         // y c2c (in place), y-Nyquist zeroed
         if (!rhs_ready) {
-            auto ca = colargs(Hx + S, lhx, S, Hx + S, lhx, S, lhx, L, 1.0, OP_FWD, ny);
+            // H_x, H_y levels 1..L in one launch, H_z levels 0..L+1 in another
+            MultiPtr<T> m{};
+            m.src[0] = m.dst[0] = Hx + S;
+            m.src[1] = m.dst[1] = Hy + S;
+            auto ca = colargs(nullptr, lhx, S, nullptr, lhx, S, lhx, L, 1.0, OP_FWD, ny);
             ca.zero_nyq = 1;
-            if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
-            ca.src = ca.dst = Hy + S;
-            if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
+            if ((rc = cols_multi(OP_FWD, ny, ca, m, 2, "press_fwd_cols"))) return rc;
             ca.src = ca.dst = Hz;
             ca.nlev = L + 2;
             if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;

@@ -828,9 +828,10 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
 template <typename T> cudaError_t launch_rows(int op, int n, const RowArgs<T> &a, cudaStream_t s);
 template <typename T> cudaError_t launch_cols(int op, bool real, int n, const ColArgs<T> &a, cudaStream_t s);
 
-// The same real-line ops (OP_DERIV, OP_PAD, OP_UNPAD) on up to kMultiFields fields of
-// one shape in one launch: field f reads src[f] and writes dst[f]; the args' src/dst are
-// ignored.  For grids whose single-field launches are too small to fill the GPU.
+// The same line ops on up to kMultiFields fields of one shape in one launch: field f
+// reads src[f] and writes dst[f]; the args' src/dst are ignored.  Rows: OP_DERIV, OP_PAD,
+// OP_UNPAD, OP_FWD; columns: the real-column OP_DERIV, OP_PAD, OP_UNPAD and the complex
+// OP_FWD.  For grids whose single-field launches are too small to fill the GPU.
 constexpr int kMultiFields = 6;
 template <typename T> struct MultiPtr {
     const void *src[kMultiFields];

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(256) k_rows_multi(RowArgs<T> a0, MultiPtr<T> m
     }
 }
 
-template <typename T, int N, int OP, int NW, int WB, bool TWG>
+template <typename T, int N, int OP, bool REAL, int NW, int WB, bool TWG>
 __global__ void __launch_bounds__(32 * NW, TWG ? 4 : 1) k_cols2_multi(ColArgs<T> a0, MultiPtr<T> m)
 {
     using C = C2<T>;
@@ -39,14 +39,14 @@ __global__ void __launch_bounds__(32 * NW, TWG ? 4 : 1) k_cols2_multi(ColArgs<T>
     a.src = m.src[f];
     a.dst = m.dst[f];
     if constexpr (TWG) {
-        cols2_unit<T, N, OP, true, NW, WB>(a, blockIdx.x, z, a.twF, a.twB, reinterpret_cast<C *>(smraw));
+        cols2_unit<T, N, OP, REAL, NW, WB>(a, blockIdx.x, z, a.twF, a.twB, reinterpret_cast<C *>(smraw));
     } else {
         C *twF = reinterpret_cast<C *>(smraw);
         C *twB = twF + D::TF;
         C *buf = twB + D::TB;
         load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
         __syncthreads();
-        cols2_unit<T, N, OP, true, NW, WB>(a, blockIdx.x, z, twF, twB, buf);
+        cols2_unit<T, N, OP, REAL, NW, WB>(a, blockIdx.x, z, twF, twB, buf);
     }
 }
 
@@ -77,7 +77,7 @@ static cudaError_t rows_multi_t(const RowArgs<T> &a, const MultiPtr<T> &m, int n
     return cudaGetLastError();
 }
 
-template <typename T, int N, int OP>
+template <typename T, int N, int OP, bool REAL>
 static cudaError_t cols_multi_t(const ColArgs<T> &a, const MultiPtr<T> &m, int nf, cudaStream_t s)
 {
     static bool inits[kMaxDevices] = {};
@@ -85,7 +85,7 @@ static cudaError_t cols_multi_t(const ColArgs<T> &a, const MultiPtr<T> &m, int n
     constexpr bool TWG = col_tw_global<T, N, OP>();
     using D = LineDerived<N, OP>;
     const size_t sm = TWG ? sizeof(C2<T>) * (size_t)D::NM * WB : cols2_smem<T, N, OP, WB>();
-    auto kern = k_cols2_multi<T, N, OP, NW, WB, TWG>;
+    auto kern = k_cols2_multi<T, N, OP, REAL, NW, WB, TWG>;
     const int ds = device_slot();
     if (ds < 0 || !inits[ds]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -94,7 +94,7 @@ static cudaError_t cols_multi_t(const ColArgs<T> &a, const MultiPtr<T> &m, int n
     }
     ColArgs<T> b = a;
     b.pf_ahead = 0;
-    const int nlines = b.ncols / 2;
+    const int nlines = REAL ? b.ncols / 2 : b.ncols;
     dim3 grid((nlines + WB - 1) / WB, (unsigned)(b.nlev * nf));
     if (grid.x < 1 || grid.y < 1) return cudaSuccess;
     kern<<<grid, 32 * NW, sm, s>>>(b, m);
@@ -108,6 +108,7 @@ static cudaError_t rows_multi_n(int op, const RowArgs<T> &a, const MultiPtr<T> &
     case OP_DERIV: return rows_multi_t<T, N, OP_DERIV>(a, m, nf, s);
     case OP_PAD: return rows_multi_t<T, N, OP_PAD>(a, m, nf, s);
     case OP_UNPAD: return rows_multi_t<T, N, OP_UNPAD>(a, m, nf, s);
+    case OP_FWD: return rows_multi_t<T, N, OP_FWD>(a, m, nf, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -116,9 +117,10 @@ template <typename T, int N>
 static cudaError_t cols_multi_n(int op, const ColArgs<T> &a, const MultiPtr<T> &m, int nf, cudaStream_t s)
 {
     switch (op) {
-    case OP_DERIV: return cols_multi_t<T, N, OP_DERIV>(a, m, nf, s);
-    case OP_PAD: return cols_multi_t<T, N, OP_PAD>(a, m, nf, s);
-    case OP_UNPAD: return cols_multi_t<T, N, OP_UNPAD>(a, m, nf, s);
+    case OP_DERIV: return cols_multi_t<T, N, OP_DERIV, true>(a, m, nf, s);
+    case OP_PAD: return cols_multi_t<T, N, OP_PAD, true>(a, m, nf, s);
+    case OP_UNPAD: return cols_multi_t<T, N, OP_UNPAD, true>(a, m, nf, s);
+    case OP_FWD: return cols_multi_t<T, N, OP_FWD, false>(a, m, nf, s);   // complex columns
     }
     return cudaErrorInvalidValue;
 }
