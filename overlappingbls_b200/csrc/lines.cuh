@@ -484,21 +484,6 @@ __device__ __forceinline__ void col_unit(const ColArgs<T> &a, int z, int tx, con
     __syncthreads();   // the tile may be reused by the caller's next unit
 }
 
-template <typename T, int N, int OP, bool REAL>
-__global__ void __launch_bounds__(256) k_cols(ColArgs<T> a)
-{
-    using C = C2<T>;
-    using E = typename std::conditional<REAL, T, C>::type;
-    using D = LineDerived<N, OP>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C *twF = reinterpret_cast<C *>(smraw);
-    C *twB = twF + D::TF;
-    E *tile = reinterpret_cast<E *>(twB + D::TB);
-    load_tables<T, N, OP>(a.twF, a.twB, twF, twB);
-    // (the first __syncthreads of col_unit orders these table writes before their use)
-    col_unit<T, N, OP, REAL>(a, blockIdx.y, blockIdx.x, twF, twB, tile);
-}
-
 // ----------------------------------------------------------------------------- line-minor columns
 // Column lines without a staging tile: a CTA owns WB adjacent complex lines (WB real
 // column pairs, or WB complex columns) of one plane.  Lane l % WB is the line and the
