@@ -134,6 +134,15 @@ int obl_divstress_uv(obl_ctx *ctx, double *divt, const double *tx, const double 
 int obl_divstress_w(obl_ctx *ctx, double *divt, const double *tx, const double *ty, const double *tz);
 int obl_divstress_uv_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz);
 int obl_divstress_w_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz);
+/* The same on z-rank `rank` of `nranks` (coordz, npz), levels 0..nz of the rank with the
+   ghost levels 0 and nz filled by the caller's exchange (103_flosol.f90:62-76): divstress_w
+   adds ddz_uv(tz) on level 1 except on rank 0, computes level nz (without it) only on the
+   top rank and leaves it BOGUS elsewhere (107_divstress.f90:81-102); divstress_uv does
+   not depend on the rank. */
+int obl_divstress_uv_slab_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz, int rank,
+                              int nranks);
+int obl_divstress_w_slab_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz, int rank,
+                             int nranks);
 
 /* ---- restart files: write_file_mpi_3d / read_file_mpi_3d (202_parallel.f90:1084-1120,
    1211-1250), checkpoint_final (012_io.f90:496-546), read_flow_field

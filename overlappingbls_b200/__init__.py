@@ -39,6 +39,7 @@ EXPORTS = [
     "obl_ddx", "obl_ddy", "obl_ddx_dev", "obl_ddy_dev",
     "obl_ddz_uv", "obl_ddz_w", "obl_ddz_uv_dev", "obl_ddz_w_dev",
     "obl_divstress_uv", "obl_divstress_w", "obl_divstress_uv_dev", "obl_divstress_w_dev",
+    "obl_divstress_uv_slab_dev", "obl_divstress_w_slab_dev",
     "obl_write_file_3d_dev", "obl_read_file_3d_dev", "obl_checkpoint_final_dev", "obl_read_flow_field_dev",
     "obl_read_total_time", "obl_write_total_time", "obl_selftest_grid_barrier",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
@@ -123,6 +124,7 @@ def load_library(path=LIB_PATH):
         "obl_ddz_uv_dev": [ctx, P, P], "obl_ddz_w_dev": [ctx, P, P],
         "obl_divstress_uv": [ctx, P, P, P, P], "obl_divstress_w": [ctx, P, P, P, P],
         "obl_divstress_uv_dev": [ctx, P, P, P, P], "obl_divstress_w_dev": [ctx, P, P, P, P],
+        "obl_divstress_uv_slab_dev": [ctx, P, P, P, P, I, I], "obl_divstress_w_slab_dev": [ctx, P, P, P, P, I, I],
         "obl_write_file_3d_dev": [ctx, P, ctypes.c_char_p, ctypes.c_longlong, I, I],
         "obl_read_file_3d_dev": [ctx, P, ctypes.c_char_p, ctypes.c_longlong, I, I],
         "obl_checkpoint_final_dev": [ctx, ctypes.c_char_p, I, ctypes.POINTER(P), I, I],
@@ -431,6 +433,14 @@ class Context:
 
     def divstress_w_dev(self, divt, tx, ty, tz):
         self._check(self._lib.obl_divstress_w_dev(self._h, divt, tx, ty, tz), "divstress_w_dev")
+
+    def divstress_uv_slab_dev(self, divt, tx, ty, tz, rank, nranks):
+        self._check(self._lib.obl_divstress_uv_slab_dev(self._h, divt, tx, ty, tz, rank, nranks),
+                    "divstress_uv_slab_dev")
+
+    def divstress_w_slab_dev(self, divt, tx, ty, tz, rank, nranks):
+        self._check(self._lib.obl_divstress_w_slab_dev(self._h, divt, tx, ty, tz, rank, nranks),
+                    "divstress_w_slab_dev")
 
     def zero_padding_dev(self, var, var_big, nlev):
         self._check(self._lib.obl_zero_padding_dev(self._h, var, var_big, nlev), "zero_padding_dev")

@@ -561,9 +561,11 @@ template <typename T> struct Ops {
     // ---- divstress_uv / divstress_w (107_divstress.f90:4-104), single-rank roles ----
     // ddx(tx) into divt's computed levels, then the ddy(ty) column pass whose stores add
     // it, the vertical difference of tz and the zero pads; BOGUS on the other levels.
-    int divstress(T *divt, const T *tx, const T *ty, const T *tz, bool w_form)
+    // bottom / top: the rank holds the wall / the top of the domain (coordz == 0 /
+    // coordz == npz-1); a whole domain holds both
+    int divstress(T *divt, const T *tx, const T *ty, const T *tz, bool w_form, bool bottom = true, bool top = true)
     {
-        const int nz = ctx->nz, nlev = w_form ? nz : nz - 1;   // levels 1..nlev
+        const int nz = ctx->nz, nlev = (w_form && top) ? nz : nz - 1;   // levels 1..nlev
         const long long pl = ctx->plane();
         auto ra = rowargs(tx + pl, ctx->ldx, divt + pl, ctx->ldx, (long long)ctx->nyt * nlev, 1.0 / ctx->nxt,
                           OP_DERIV, ctx->nxt);
@@ -581,8 +583,8 @@ template <typename T> struct Ops {
         ep.ncols = ctx->nxt;
         ep.rdz = (T)(1.0 / ctx->dz);
         ep.fwd = w_form ? 0 : 1;
-        ep.zlo = w_form ? 1 : 0;            // divstress_w: no dz(tzz) on the wall level (:81-85)
-        ep.zhi = w_form ? nz - 2 : nlev - 1; // ... nor on the top level (:97-98)
+        ep.zlo = (w_form && bottom) ? 1 : 0;  // divstress_w: no dz(tzz) on the wall level (:81-88)
+        ep.zhi = w_form ? nz - 2 : nlev - 1;  // ... nor on the top level (:97-98)
         {
             LaunchScope ls(ctx->rec, "divt_ddy_cols", s());
             if ((rc = chk(launch_cols_divt<T>(ctx->nyt, ca, ep, s()), "divt_ddy_cols"))) return rc;
@@ -590,7 +592,7 @@ template <typename T> struct Ops {
         cudaError_t e = cudaSuccess;
         LaunchScope ls(ctx->rec, "divt_bogus", s());
         launch_fill<T>(divt, pl, (T)-1234567890.0, s(), e);   // BOGUS, 001_param.f90:40
-        if (!w_form) launch_fill<T>(divt + pl * nz, pl, (T)-1234567890.0, s(), e);
+        if (!w_form || !top) launch_fill<T>(divt + pl * nz, pl, (T)-1234567890.0, s(), e);   // :42, :101
         return chk(e, "divt_bogus");
     }
 
@@ -1603,6 +1605,22 @@ int obl_divstress_w_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty
 {
     if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2) return OBL_ERR_ARG;
     DEVCALL(ctx, return o.divstress((T *)divt, (const T *)tx, (const T *)ty, (const T *)tz, true););
+}
+int obl_divstress_uv_slab_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz, int rank,
+                              int nranks)
+{
+    if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2 || nranks < 1 || rank < 0 || rank >= nranks)
+        return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.divstress((T *)divt, (const T *)tx, (const T *)ty, (const T *)tz, false, rank == 0,
+                                    rank == nranks - 1););
+}
+int obl_divstress_w_slab_dev(obl_ctx *ctx, void *divt, const void *tx, const void *ty, const void *tz, int rank,
+                             int nranks)
+{
+    if (!ctx || !divt || !tx || !ty || !tz || ctx->nz < 2 || nranks < 1 || rank < 0 || rank >= nranks)
+        return OBL_ERR_ARG;
+    DEVCALL(ctx, return o.divstress((T *)divt, (const T *)tx, (const T *)ty, (const T *)tz, true, rank == 0,
+                                    rank == nranks - 1););
 }
 
 int obl_write_file_3d_dev(obl_ctx *ctx, const void *var, const char *fn, long long disp0, int zrank, int nzranks)

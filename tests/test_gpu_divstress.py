@@ -151,3 +151,44 @@ def test_divstress_512_full_size():
                       f"{16 * pts / ms / 1e6:.0f} GB/s algorithmic (16 B/pt)")
     print("; ".join(report))
     ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("form", ["uv", "w"])
+def test_divstress_z_ranks_match_whole_domain(prec, form):
+    """z-rank roles (107_divstress.f90:81-102): two ranks, each holding its levels with the
+    ghost levels 0 and nz from its neighbours, give the whole-domain result on every level
+    they compute; rank 0 leaves the wall level without dz(tzz), only the top rank computes
+    level nz of divstress_w, and the others leave it BOGUS."""
+    import torch
+    from overlappingbls_b200 import slab
+    nx, ny, P, Lr = 64, 48, 2, 8
+    nzt = P * Lr + 1
+    whole = obl.Context(nx, ny, nzt, precision=prec, **fields.DOMAIN)
+    t = _stress(nx, ny, nzt, prec, seed=11)
+    ref = whole.field()
+    getattr(whole, "divstress_" + form)(ref, t["tx"], t["ty"], t["tz"])
+    whole.close()
+    nzt_r, lz_r = slab.slab_grid(nx, ny, nzt, fields.DOMAIN["lz_tot"], P)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    b = BOGUS if prec == "f64" else float(np.float32(BOGUS))
+    tol = 1e-14 if prec == "f64" else 1e-6
+    for r in range(P):
+        ctx = obl.Context(nx, ny, nzt_r, precision=prec, **dict(fields.DOMAIN, lz_tot=lz_r))
+        nz = ctx.nz
+        loc = {k: torch.from_numpy(np.asfortranarray(v[:, :, r * Lr: r * Lr + nz + 1]).ravel(order="F")).to("cuda", dt)
+               for k, v in t.items()}
+        out = torch.full(((nx + 2) * ny * (nz + 1),), 5.0, dtype=dt, device="cuda")
+        getattr(ctx, "divstress_" + form + "_slab_dev")(out.data_ptr(), loc["tx"].data_ptr(), loc["ty"].data_ptr(),
+                                                        loc["tz"].data_ptr(), r, P)
+        ctx.synchronize()
+        got = out.double().cpu().numpy().reshape((nx + 2, ny, nz + 1), order="F")
+        top = r == P - 1
+        lv = list(range(1, nz + 1)) if (form == "w" and top) else list(range(1, nz))
+        gl = [r * Lr + k for k in lv]
+        assert rel_l2(got[:nx, :, lv], ref[:nx, :, gl]) <= tol, r
+        assert np.all(got[nx:, :, lv] == 0.0)
+        assert np.all(got[:, :, 0] == b)
+        if not (form == "w" and top):
+            assert np.all(got[:, :, nz] == b)
+        ctx.close()
