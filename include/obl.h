@@ -186,21 +186,26 @@ int obl_zero_padding_dev(obl_ctx *ctx, const void *var, void *var_big, int nlev)
 int obl_zero_unpadding_dev(obl_ctx *ctx, const void *var_big, void *var, int nlev);
 
 /* ---- zero_padding that allocates nothing (no counterpart in the reference) ----
-   For callers that cannot allocate device memory when they call: code running while a
-   CUDA graph is being captured, or an application that reserves all device memory at
-   start-up and forbids allocation afterwards.  Same arguments and result as
-   obl_zero_padding_dev, but the intermediate x-padded plane lives in a static device
-   array of OBL_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
-   the process exits; the call itself performs no cudaMalloc/cudaFree.
+   For callers that cannot allocate device memory when they call: an application that
+   hands all device memory to its own pool at start-up and forbids allocation afterwards
+   (a time loop that sized its fields once), or code on a latency-critical path where
+   cudaMalloc may block and cudaFree waits for the whole device.  Same arguments and
+   result as obl_zero_padding_dev, but the intermediate x-padded plane lives in a static
+   device array of OBL_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
+   until the process exits; the call itself performs no cudaMalloc/cudaFree.
    - Sizes: es * nxt2 * nyt * nlev must fit in OBL_NOALLOC_SCRATCH_BYTES (es = 8 for
      OBL_PREC_F64, 4 otherwise); larger requests return OBL_ERR_ARG with an explanation
      in obl_last_error (pass fewer levels per call).
    - The first call on a device looks up the array's device address
-     (cudaGetSymbolAddress) with that device current; make that first call before any
-     stream capture.
+     (cudaGetSymbolAddress) with that device current and keeps it for the process; make
+     that first call before any stream capture.  A cudaDeviceReset of that device
+     invalidates the kept address (and every context on the device): do not call this
+     entry point again after one.
    - All calls share the one array: calls that overlap on the GPU (different streams or
-     contexts without ordering) race on it.  Every element of the scratch is rewritten
-     before it is read, so nothing needs clearing between calls. */
+     contexts without ordering) race on it, so serialise them on one stream.  Every
+     element of the scratch is rewritten before it is read, so nothing needs clearing
+     between calls.
+   - The caller's current device is restored on return. */
 #define OBL_NOALLOC_SCRATCH_BYTES (8u << 20)
 int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void *var_big, int nlev);
 

@@ -255,12 +255,21 @@ class Grid:
         lib().orc_project(self.ref, _p(u), _p(v), _p(w), _p(dpdx), _p(dpdy), _p(dpdz))
         return u, v, w
 
-    def step(self, u, v, w, theta, npz=1):
-        u, v, w = (np.array(a, order="F", copy=True) for a in (u, v, w))
-        d = [self.field() for _ in range(8)]
-        big = [np.zeros((self.nxt2, self.nyt2, self.nz + 1), order="F") for _ in range(4)]
-        p = self.field()
-        dp = [self.dfield() for _ in range(3)]
+    def step_outputs(self):
+        """Output arrays of step(), allocated once so that repeated steps reuse them."""
+        return dict(u=self.field(), v=self.field(), w=self.field(), d=[self.field() for _ in range(8)],
+                    big=[np.zeros((self.nxt2, self.nyt2, self.nz + 1), order="F") for _ in range(4)],
+                    p=self.field(), dpdx=self.dfield(), dpdy=self.dfield(), dpdz=self.dfield())
+
+    def step(self, u, v, w, theta, npz=1, out=None):
+        """One step; out (from step_outputs) receives the results instead of new arrays."""
+        if out is None:
+            out = self.step_outputs()
+        for k, a in (("u", u), ("v", v), ("w", w)):
+            out[k][...] = a
+        u, v, w = out["u"], out["v"], out["w"]
+        d, big, p = out["d"], out["big"], out["p"]
+        dp = [out["dpdx"], out["dpdy"], out["dpdz"]]
         D = (ctypes.c_void_p * 8)(*[a.ctypes.data for a in d])
         B = (ctypes.c_void_p * 4)(*[a.ctypes.data for a in big])
         DP = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in dp])

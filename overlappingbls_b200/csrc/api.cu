@@ -2162,11 +2162,12 @@ int obl_rollout_grad(obl_ctx *ctx, int nsteps, const double *u0, const double *v
 } // extern "C"
 
 // ============================================================================= no-allocation variant
-// Some callers cannot allocate device memory at call time: code that runs while a CUDA
-// graph is being captured, or an application that reserves all device memory up front
-// and forbids allocation afterwards.  For them zero_padding has one variant whose
-// intermediate x-padded plane lives in a fixed-size static device array instead of a
-// buffer that the context allocates on first use.  The array is part of the module
+// Some callers cannot allocate device memory at call time: an application that hands all
+// device memory to its own pool at start-up and forbids allocation afterwards (a time loop
+// that sized its fields once), or code on a latency-critical path where cudaMalloc may
+// block and cudaFree waits for the whole device.  For them zero_padding has one variant
+// whose intermediate x-padded plane lives in a fixed-size static device array instead of
+// a buffer that the context allocates on first use.  The array is part of the module
 // image, so every GPU that loads this library holds OBL_NOALLOC_SCRATCH_BYTES until the
 // process exits.
 namespace {
@@ -2205,14 +2206,19 @@ extern "C" int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void 
                     "zero_padding_noalloc: " + std::to_string(nlev) + " level(s) need " + std::to_string(need) +
                         " bytes of scratch but the static scratch holds " + std::to_string(kNoAllocBytes) +
                         " bytes; pass fewer levels per call");
+    // the caller's current device is put back on return
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
     if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice");
     void *xb = nullptr;
-    const int rc = noalloc_scratch(ctx, &xb);
-    if (rc) return rc;
-    return dispatchT(ctx, [&](auto &o) -> int {
-        using T = typename std::remove_reference<decltype(o)>::type::Tt;
-        return o.pad_with_scratch((const T *)var, (T *)var_big, (T *)xb, nlev);
-    });
+    int rc = noalloc_scratch(ctx, &xb);
+    if (!rc)
+        rc = dispatchT(ctx, [&](auto &o) -> int {
+            using T = typename std::remove_reference<decltype(o)>::type::Tt;
+            return o.pad_with_scratch((const T *)var, (T *)var_big, (T *)xb, nlev);
+        });
+    if (prev >= 0 && prev != ctx->dev) cudaSetDevice(prev);
+    return rc;
 }
 
 // ============================================================================= ensemble

@@ -1,6 +1,7 @@
 """GPU test of obl_zero_padding_noalloc_dev, the zero_padding variant that allocates
-nothing (for callers that may not allocate device memory when they call, e.g. while a
-CUDA graph is being captured).  Its scratch is a static device array, so the test
+nothing (for callers that may not allocate device memory when they call: an application
+whose device memory all belongs to its own pool, or a latency-critical path where
+cudaMalloc/cudaFree would block).  Its scratch is a static device array, so the test
 checks, through the C ABI, that two calls in a row give the same result as the
 allocating entry point obl_zero_padding_dev, that the calls do not change the free
 device memory, and that a request larger than the static scratch is refused.
