@@ -7,6 +7,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -82,6 +83,7 @@ struct obl_ctx {
     long long param_fwd_clusters = 16;  // clusters of the fused forward kernel (0 = all resident)
     long long param_fwd_csize = 8;      // CTAs per cluster
     long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
+    long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t ev[9] = {};
@@ -118,13 +120,26 @@ static int cuda_fail(obl_ctx *c, cudaError_t e, const char *where)
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, "cudaSetDevice");                         \
     } while (0)
 
+// Every device allocation of a context goes through here.  The "fail_alloc" parameter
+// (obl_set_param) or, for the allocations of obl_ctx_create, the OBL_FAIL_ALLOC
+// environment variable makes the n-th allocation from then on fail as cudaMalloc would,
+// so that the OBL_ERR_NOMEM paths can be tested on the host side; off (0) by default.
+static cudaError_t dev_malloc(obl_ctx *ctx, void **p, size_t bytes)
+{
+    if (ctx && ctx->param_fail_alloc > 0 && --ctx->param_fail_alloc == 0) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
 static int ensure(obl_ctx *ctx, DevBuf &b, size_t bytes)
 {
     if (b.n >= bytes) return OBL_OK;
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.n = 0;
-    if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+    if (dev_malloc(ctx, &b.p, bytes) != cudaSuccess) {
         cudaGetLastError();
         return fail(ctx, OBL_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
     }
@@ -545,6 +560,8 @@ template <typename T> struct Ops {
     int io_reserve()
     {
         const size_t plane = (size_t)ctx->nxt * ctx->nyt, chunk = (size_t)8 << 20;   // 64 MiB of doubles
+        if (ctx->param_fail_alloc > 0 && --ctx->param_fail_alloc == 0)
+            return fail(ctx, OBL_ERR_NOMEM, "restart staging: allocation failed");
         return io_stage_reserve(ctx->io, chunk > plane ? chunk : plane, ctx->err);
     }
     int write_field(const T *var, int fd, long long off)
@@ -1277,6 +1294,7 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
         obl_ctx_destroy(ctx);
         return code;
     };
+    if (const char *fa = std::getenv("OBL_FAIL_ALLOC")) ctx->param_fail_alloc = std::atoll(fa);
     if (cudaSetDevice(ctx->dev) != cudaSuccess) return bad(OBL_ERR_CUDA);
 
     // wavenumbers (002_fft.f90:131-165)
@@ -1289,7 +1307,7 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
         ky2[j] = (((double)(((j + ctx->nyt / 2) % ctx->nyt) - ctx->nyt / 2) * 2.0) * kPi) / ctx->ly;
     ky2[ctx->nyt / 2] = 0.0;
     auto upload = [&](double **d, const std::vector<double> &h) {
-        if (cudaMalloc(d, sizeof(double) * h.size()) != cudaSuccess) return false;
+        if (dev_malloc(ctx, (void **)d, sizeof(double) * h.size()) != cudaSuccess) return false;
         return cudaMemcpy(*d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
     };
     if (!upload(&ctx->d_kx, kx) || !upload(&ctx->d_ky1, ky1) || !upload(&ctx->d_ky2, ky2)) return bad(OBL_ERR_NOMEM);
@@ -1304,7 +1322,7 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
             const size_t m = h.size() / 2;
             const size_t b = (ctx->f64 ? sizeof(double2) : sizeof(float2)) * (m > 0 ? m : 1);
             void *d = nullptr;
-            if (cudaMalloc(&d, b) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            if (dev_malloc(ctx, &d, b) != cudaSuccess) return bad(OBL_ERR_NOMEM);
             ctx->tw[key] = d;
             if (m == 0) continue;
             if (ctx->f64) {
@@ -1339,14 +1357,16 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
         if (ctx->n_isl) {
             std::vector<int> slot(skip.size(), -1);
             for (size_t k = 0; k < cols.size(); ++k) slot[(size_t)cols[k]] = (int)k;
-            if (cudaMalloc(&ctx->d_isl, sizeof(int) * cols.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
-            if (cudaMalloc(&ctx->d_skip, skip.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
-            if (cudaMalloc(&ctx->d_isl_slot, sizeof(int) * slot.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            if (dev_malloc(ctx, (void **)&ctx->d_isl, sizeof(int) * cols.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            if (dev_malloc(ctx, (void **)&ctx->d_skip, skip.size()) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+            if (dev_malloc(ctx, (void **)&ctx->d_isl_slot, sizeof(int) * slot.size()) != cudaSuccess)
+                return bad(OBL_ERR_NOMEM);
             cudaMemcpy(ctx->d_isl, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice);
             cudaMemcpy(ctx->d_skip, skip.data(), skip.size(), cudaMemcpyHostToDevice);
             cudaMemcpy(ctx->d_isl_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice);
         }
     }
+    ctx->param_fail_alloc = 0;   // OBL_FAIL_ALLOC applies to the creation only
     *out = ctx;
     return OBL_OK;
 }
@@ -1434,6 +1454,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "fwd_clusters")) return &ctx->param_fwd_clusters;
     if (!std::strcmp(name, "fwd_cluster_size")) return &ctx->param_fwd_csize;
     if (!std::strcmp(name, "tdma_segments")) return &ctx->param_tdma_segments;
+    if (!std::strcmp(name, "fail_alloc")) return &ctx->param_fail_alloc;
     return nullptr;
 }
 

@@ -20,7 +20,7 @@ private
 public :: obl_gpu_init, obl_gpu_finalize, ddx_gpu, ddy_gpu, ddz_uv_gpu, ddz_w_gpu, &
           divstress_uv_gpu, divstress_w_gpu, &
           zero_padding_gpu, zero_unpadding_gpu, filter_data_gpu, fftn_gpu, ifftn_gpu, &
-          press_stag_array_gpu, dpdz_gpu, project_gpu, obl_gpu_check
+          press_stag_array_gpu, press_stag_array_planes_gpu, dpdz_gpu, project_gpu, obl_gpu_check
 
 integer(c_int), parameter, public :: OBL_PREC_F64 = 0, OBL_PREC_MIXED = 1, OBL_PREC_F32 = 2
 integer(c_int), parameter, public :: OBL_TOP_SINGLE_RANK = 0, OBL_TOP_NEUMANN = 1
@@ -265,6 +265,18 @@ subroutine press_stag_array_gpu(func, dfdx, dfdy, u, v, w, divtz)
     real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(in) :: u, v, w, divtz
     call obl_gpu_check(obl_press_stag_array(ctx, u, v, w, divtz(:, :, 1), divtz(:, :, g_nz), &
                                             func, dfdx, dfdy), 'press_stag_array')
+end subroutine
+
+! The same with the two divtz boundary planes given separately, for a caller that has
+! already folded the surface-temperature term of 109_press_stag_array.f90:187-192 into
+! the bottom plane (obl_dropin.f90).
+subroutine press_stag_array_planes_gpu(func, dfdx, dfdy, u, v, w, divtz_bot, divtz_top)
+    real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(out) :: func
+    real(c_double), dimension(g_ldx, g_nyt, g_nz), intent(out) :: dfdx, dfdy
+    real(c_double), dimension(g_ldx, g_nyt, 0:g_nz), intent(in) :: u, v, w
+    real(c_double), dimension(g_ldx, g_nyt), intent(in) :: divtz_bot, divtz_top
+    call obl_gpu_check(obl_press_stag_array(ctx, u, v, w, divtz_bot, divtz_top, func, dfdx, dfdy), &
+                       'press_stag_array')
 end subroutine
 
 subroutine dpdz_gpu(dpdz, p)                   ! 103_flosol.f90:174-175

@@ -82,11 +82,20 @@ class SlabStep:
     def above(self):
         return self.planes[self.rank + 1] if self.rank < self.nranks - 1 else None
 
+    def _gather(self, what, out, inp):
+        # a rank that left or stalls ends the survivors' collective with the process
+        # group's timeout or a closed connection; say which exchange of the step it was
+        try:
+            self.comm.all_gather(out, inp)
+        except Exception as e:
+            raise RuntimeError(f"slab step, rank {self.rank} of {self.nranks}: the all-gather of the {what} "
+                               f"failed ({type(e).__name__}: {e})") from e
+
     def step(self, io):
         self.b.begin(io, self.rank, self.nranks, self.plane)
-        self.comm.all_gather(self.planes, self.plane)
+        self._gather("H_z(1) planes", self.planes, self.plane)
         self.b.solve(self.above(), self.rank, self.nranks, self.iface)
-        self.comm.all_gather(self.ifaces, self.iface)
+        self._gather("interface coefficients", self.ifaces, self.iface)
         self.b.finish(io, self.ifaces, self.rank, self.nranks)
 
 

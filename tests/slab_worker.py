@@ -83,3 +83,52 @@ def run(rank, world, port, out_path):
             np.save(out_path, allp.numpy())
     finally:
         dist.destroy_process_group()
+
+
+class LeavingComm:
+    """TorchComm whose rank `who` leaves before its second all-gather: it exits the
+    process abruptly ("exit"), or stops taking part and sleeps ("stall")."""
+
+    def __init__(self, comm, who, how, stall_s):
+        self.c, self.who, self.how, self.stall_s, self.calls = comm, who, how, stall_s, 0
+
+    def all_gather(self, out, inp):
+        self.calls += 1
+        if self.calls == 2 and self.c.rank == self.who:
+            if self.how == "exit":
+                os._exit(0)
+            import time
+            time.sleep(self.stall_s)
+            os._exit(0)
+        self.c.all_gather(out, inp)
+
+
+def run_leaving(rank, world, port, out_path, how, timeout_s):
+    """One slab step with rank world-1 leaving before the second all-gather; every other
+    rank records (error message, seconds spent in the step) in out_path.<rank>.json."""
+    import datetime
+    import json
+    import time
+    import torch.distributed as dist
+    from overlappingbls_b200 import slab
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=timeout_s))
+    g, tables, H = problem()
+    L = H[0].shape[1] - 2
+    Lr = L // world
+    sl = slice(rank * Lr, rank * Lr + Lr + 2)
+    io = {"H": [h[:, sl].copy() for h in H]}
+    b = NumpyBackend(tables, g.dz)
+    b.io = io
+    comm = LeavingComm(slab.TorchComm(), world - 1, how, stall_s=3 * timeout_s + 10)
+    step = slab.SlabStep(b, rank, world, comm)
+    t0 = time.monotonic()
+    err = None
+    try:
+        step.step(io)
+    except Exception as e:
+        err = str(e)
+    rec = {"error": err, "seconds": time.monotonic() - t0}
+    with open(f"{out_path}.{rank}.json", "w") as fh:
+        json.dump(rec, fh)
+    os._exit(0)   # the group is broken: leave without its teardown collective
