@@ -515,13 +515,19 @@ template <typename T, int NW_ = 8, int WB_ = (sizeof(T) == 4 ? 8 : 4)> struct Lm
 #ifndef OBL_PAD_WB
 #define OBL_PAD_WB 8
 #endif
+#ifndef OBL_COLS_NW
+#define OBL_COLS_NW 8   // warps per CTA of the FP32 ddy / forward y-transform of long lines
+#endif
+#ifndef OBL_COLS_WB
+#define OBL_COLS_WB 8   // lines per CTA of the same
+#endif
 #ifndef OBL_COL_PF
 #define OBL_COL_PF 2   // y-pad column kernel: L2 prefetch distance in quarters of a residency window (0 = off)
 #endif
 template <typename T, int N, int OP> constexpr int col_warps()
 {
     return (sizeof(T) == 4 && N >= 256) ? (OP == OP_PAD ? OBL_PAD_NW
-                                                        : ((OBL_COLS_TWG && (OP == OP_DERIV || OP == OP_FWD)) ? 8 : 16))
+                                                        : ((OBL_COLS_TWG && (OP == OP_DERIV || OP == OP_FWD)) ? OBL_COLS_NW : 16))
                                         : 8;
 }
 // Twiddles read through L1 instead of staged in shared memory, with the registers bounded
@@ -538,8 +544,14 @@ template <typename T, int N, int OP> constexpr bool col_tw_global()
 // lines per CTA of the standalone column kernels (build-time knob for the FP32 y-pad)
 template <typename T, int N, int OP> constexpr int col_lines()
 {
-    return (sizeof(T) == 4 && N >= 256 && OP == OP_PAD) ? OBL_PAD_WB : LmGeo<T>::WB;
+    return (sizeof(T) == 4 && N >= 256 && OP == OP_PAD)
+               ? OBL_PAD_WB
+               : ((sizeof(T) == 4 && N >= 256 && OBL_COLS_TWG && (OP == OP_DERIV || OP == OP_FWD)) ? OBL_COLS_WB
+                                                                                                 : LmGeo<T>::WB);
 }
+// Minimum resident CTAs per SM the column kernels are compiled for: with twiddles through
+// L1, registers are bounded so that the CTAs of 32 warps in total fit on an SM.
+constexpr int col_min_blocks(int nw, bool twg) { return twg ? (nw >= 32 ? 1 : 32 / nw) : 1; }
 
 template <typename T, int N, int OP, int NW = 8, int WB = LmGeo<T>::WB> struct ColDerived {
     using D = LineDerived<N, OP>;
@@ -716,7 +728,7 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
 }
 
 template <typename T, int N, int OP, bool REAL, int NW, int WB, bool TWG = false>
-__global__ void __launch_bounds__(32 * NW, TWG ? 4 : 1) k_cols2(ColArgs<T> a)
+__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG)) k_cols2(ColArgs<T> a)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP>;
