@@ -207,6 +207,7 @@ def algorithmic_bytes(name, info, s):
         "press_fwd_cols": 2 * lhx * ny * L * c,
         "tdma": 5 * lhx * ny * L * c,
         "tdma_mixed": 5 * lhx * ny * L * c,
+        "tdma_reg": 5 * lhx * ny * L * c,
         # one launch per field: field in, ddx and the x-padded rows out, and on u, v, w the
         # RHS x-spectrum of levels 1..L out (mean over the 4 launches of a step)
         "rows_fwd3": ((2 * nx + nx2) * ny * nlev * s * 4 + 3 * lhx * ny * L * c) / 4,

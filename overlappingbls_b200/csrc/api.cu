@@ -84,6 +84,7 @@ struct obl_ctx {
     long long param_fwd_csize = 8;      // CTAs per cluster
     long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
+    long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t ev[9] = {};
@@ -469,7 +470,25 @@ template <typename T> struct Ops {
             if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_seg");
         } else {
             cudaError_t e = cudaSuccess;
-            if (ctx->n_isl) {
+            bool done = false;
+            if constexpr (std::is_same<T, float>::value) {
+                if (ctx->param_tdma_reg && tdma_reg_supported(L)) {
+                    // FP32 bulk columns by the register-segmented solve, FP64 islands by
+                    // their sequential sweep, in one launch
+                    IslandArgs isl{nullptr, 0, nullptr, nullptr};
+                    if (ctx->n_isl) {
+                        if ((rc = ensure(ctx, ctx->isl_c, sizeof(double) * (size_t)ctx->n_isl * L))) return rc;
+                        if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
+                        isl = IslandArgs{ctx->d_isl, ctx->n_isl, (double *)ctx->isl_c.p, (double2 *)ctx->isl_d.p};
+                    }
+                    LaunchScope ls(ctx->rec, "tdma_reg", s());
+                    launch_tdma_reg<float>(ta, isl, s(), e);
+                    if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_reg");
+                    done = true;
+                }
+            }
+            if (done) {
+            } else if (ctx->n_isl) {
                 // FP32 bulk and FP64 island columns in one launch
                 if ((rc = ensure(ctx, ctx->isl_c, sizeof(double) * (size_t)ctx->n_isl * L))) return rc;
                 if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
@@ -1455,6 +1474,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "fwd_cluster_size")) return &ctx->param_fwd_csize;
     if (!std::strcmp(name, "tdma_segments")) return &ctx->param_tdma_segments;
     if (!std::strcmp(name, "fail_alloc")) return &ctx->param_fail_alloc;
+    if (!std::strcmp(name, "tdma_reg")) return &ctx->param_tdma_reg;
     return nullptr;
 }
 

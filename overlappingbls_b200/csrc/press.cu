@@ -61,6 +61,220 @@ void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_
     e = cudaGetLastError();
 }
 
+// ----------------------------------------------------------------------------- register-segmented solve
+// The FP32 bulk columns without scratch traffic.  A CTA owns 32 consecutive columns
+// (lane = column, so every load and store of a level is 256 contiguous bytes) and splits
+// their L rows into kRegSeg segments of Ls <= kRegLev rows, one warp per segment.  Each
+// thread eliminates its segment's rows with the neighbouring segments' boundary values
+// left as unknowns (the partition method: x_i = y_i + v_i x_{s-1} + w_i x_{e+1}), keeping
+// the forward sweep's y', v', c' in registers; lane l of warp 0 then solves column l's
+// reduced system of 2K boundary values (a 2x2-block tridiagonal chain, eliminated upward
+// and substituted downward) in shared memory, and every thread back-substitutes its rows
+// from registers.  HBM sees only the compulsory traffic: three RHS spectra in, p_hat and
+// the dpdz spectrum out (the one-sweep solve also writes and re-reads c' and d').
+// The bands, RHS and boundary rows are those of tdma_column (109_press_stag_array.f90:
+// 4-63, 203-225, 280-317); the rows are the same, only the elimination order differs.
+// FP64 island columns keep the sequential FP64 sweep, in the launch's first nbi blocks.
+constexpr int kRegSeg = 16;   // warps per CTA = segments per column
+constexpr int kRegLev = 16;   // rows a segment keeps in registers (so L <= 256)
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kRegSeg, 1) k_tdma_reg(TdmaArgs<T> a, IslandArgs isl, int nbi, int Ls, int K)
+{
+    using C = C2<T>;
+    if ((int)blockIdx.x < nbi) {
+        tdma_column<T, double, true>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+        return;
+    }
+    // boundary coefficients of every segment (x_s = Ys + Vs x_{s-1} + Ws x_{e+1}, same for
+    // x_e), the reduced elimination (x_s^j = S_j + T_j x_s^{j+1}, x_e^j = P_j + Q_j x_s^{j+1})
+    // and the solved boundary values
+    __shared__ C sYs[kRegSeg][32], sYe[kRegSeg][32], sS[kRegSeg][32], sP[kRegSeg][32];
+    __shared__ C sXs[kRegSeg][32], sXe[kRegSeg][32];
+    __shared__ T sVs[kRegSeg][32], sVe[kRegSeg][32], sWs[kRegSeg][32], sWe[kRegSeg][32];
+    __shared__ T sT[kRegSeg][32], sQ[kRegSeg][32];
+    const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+    const long long S = a.S;
+    const int L = a.L;
+    const long long q = (long long)(blockIdx.x - nbi) * 32 + lane;
+    const bool inq = q < S;
+    const int ix = inq ? (int)(q % a.lhx) : 0, iy = inq ? (int)(q / a.lhx) : 0;
+    const bool nyq = inq && (ix == a.lhx - 1 || iy == a.nyt / 2);
+    const bool isl_col = inq && a.skip && a.skip[q];
+    const bool act = inq && !nyq && !isl_col;
+    const int s = 1 + k * Ls;                                   // first row of the segment
+    const int ns = k < K ? min(Ls, L - s + 1) : 0;              // its rows (0: idle warp)
+    C *ph = a.phat + q;
+    C *dph = a.dph ? a.dph + q : nullptr;
+
+    // Nyquist columns: p_hat = 0 at every level (:303-305)
+    if (nyq && ns > 0) {
+        for (int i = 0; i < ns; ++i) {
+            ph[S * (s + i)] = mk<T>(0, 0);
+            if (dph) dph[S * (s + i)] = mk<T>(0, 0);
+        }
+        if (k == 0) ph[0] = mk<T>(0, 0);
+    }
+
+    const double kxd = act ? a.kx[ix] : 0.0, kyd = act ? a.ky[iy] : 0.0;
+    const double k2d = kxd * kxd + kyd * kyd;   // 002_fft.f90:167
+    const bool m00 = (k2d == 0.0);
+    const T kx = (T)kxd, ky = (T)kyd, k2 = (T)k2d;
+    const T dz = (T)a.dz, idz = (T)(1.0 / a.dz), idz2 = (T)(1.0 / (a.dz * a.dz));
+    const bool top_solved = a.neumann_top;      // else row L is p_hat(L) = 0 (npz = 1 mode)
+
+    C y[kRegLev];
+    T cp[kRegLev], vp[kRegLev];
+    C hz0 = mk<T>(0, 0);
+    if (act && ns > 0) {
+        // right-hand sides of rows s..s+ns-1, all loads independent (:203-225)
+        if (k == 0) hz0 = a.Hz[q];   // RHS_col(0) = H_z(0) (:209)
+        C hz[kRegLev + 1];
+#pragma unroll
+        for (int i = 0; i <= kRegLev; ++i)
+            if (i <= ns) hz[i] = a.Hz[q + S * (s + i)];
+#pragma unroll
+        for (int i = 0; i < kRegLev; ++i) {
+            if (i < ns) {
+                const int iz = s + i;
+                C r;
+                if (!m00) {
+                    const C hx = a.Hx[q + S * iz], hy = a.Hy[q + S * iz];
+                    const C sxy = mk<T>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
+                    C dh = csub(hz[i + 1], hz[i]);
+                    if (iz == 1) dh = cadd(dh, hz0);
+                    r = mk<T>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+                } else {
+                    r = (iz == 1) ? mk<T>(0, 0) : hz[i];
+                }
+                if (iz == L && !top_solved) r = mk<T>(0, 0);
+                y[i] = r;
+            }
+        }
+        // forward sweep with x_{s-1} left unknown: x_i = y'_i + v'_i x_{s-1} - c'_i x_{i+1}
+        T cprev = 0, vprev = 1;
+        C yprev = mk<T>(0, 0);
+#pragma unroll
+        for (int i = 0; i < kRegLev; ++i) {
+            if (i < ns) {
+                const int iz = s + i;
+                T am, bm, cm;
+                if (iz == L && !top_solved) {
+                    am = 0; bm = 1; cm = 0;
+                } else if (!m00) {
+                    const bool top = iz == L;   // the Neumann top row (:33-38 with npz >= 2)
+                    am = (iz == 1) ? (T)0 : idz2;
+                    bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (T)2 * idz2);
+                    cm = top ? (T)0 : idz2;
+                } else {
+                    am = (iz == 1) ? (T)0 : -idz;
+                    bm = idz;
+                    cm = 0;
+                }
+                const T ibp = (T)1 / (bm - am * cprev);
+                cp[i] = cm * ibp;
+                vp[i] = -am * vprev * ibp;
+                y[i] = mk<T>((y[i].x - am * yprev.x) * ibp, (y[i].y - am * yprev.y) * ibp);
+                cprev = cp[i];
+                vprev = vp[i];
+                yprev = y[i];
+            }
+        }
+        // the segment's two boundary rows in terms of x_{s-1} and x_{e+1}
+        C ys = y[0];
+        T vs = 0, ws = 0;
+#pragma unroll
+        for (int i = kRegLev - 1; i >= 0; --i) {
+            if (i == ns - 1) {
+                ys = y[i];
+                vs = vp[i];
+                ws = -cp[i];
+                sYe[k][lane] = ys;
+                sVe[k][lane] = vs;
+                sWe[k][lane] = ws;
+            } else if (i < ns - 1) {
+                ys = mk<T>(y[i].x - cp[i] * ys.x, y[i].y - cp[i] * ys.y);
+                vs = vp[i] - cp[i] * vs;
+                ws = -cp[i] * ws;
+            }
+        }
+        sYs[k][lane] = ys;
+        sVs[k][lane] = vs;
+        sWs[k][lane] = ws;
+    }
+    __syncthreads();
+    if (k == 0 && act) {
+        // reduced system: x_e^{j-1} = P + Q x_s^j eliminated upward, then substituted down
+        C P = mk<T>(0, 0);
+        T Q = 0;
+        for (int j = 0; j < K; ++j) {
+            const C ys = sYs[j][lane], ye = sYe[j][lane];
+            const T vs = sVs[j][lane], ws = sWs[j][lane], ve = sVe[j][lane], we = sWe[j][lane];
+            const T iden = (T)1 / ((T)1 - vs * Q);
+            const C Sj = mk<T>((ys.x + vs * P.x) * iden, (ys.y + vs * P.y) * iden);
+            const T Tj = ws * iden;
+            const C Pj = mk<T>(ye.x + ve * (P.x + Q * Sj.x), ye.y + ve * (P.y + Q * Sj.y));
+            const T Qj = ve * Q * Tj + we;
+            sS[j][lane] = Sj;
+            sT[j][lane] = Tj;
+            sP[j][lane] = Pj;
+            sQ[j][lane] = Qj;
+            P = Pj;
+            Q = Qj;
+        }
+        C xs = sS[K - 1][lane];          // the top segment has no x_{e+1} (c = 0 in its last row)
+        sXs[K - 1][lane] = xs;
+        sXe[K - 1][lane] = sP[K - 1][lane];
+        for (int j = K - 2; j >= 0; --j) {
+            const T Tj = sT[j][lane], Qj = sQ[j][lane];
+            const C Sj = sS[j][lane], Pj = sP[j][lane];
+            sXe[j][lane] = mk<T>(Pj.x + Qj * xs.x, Pj.y + Qj * xs.y);
+            xs = mk<T>(Sj.x + Tj * xs.x, Sj.y + Tj * xs.y);
+            sXs[j][lane] = xs;
+        }
+    }
+    __syncthreads();
+    if (!act || ns == 0) return;
+    const C xl = k > 0 ? sXe[k - 1][lane] : mk<T>(0, 0);
+    const C xr = k < K - 1 ? sXs[k + 1][lane] : mk<T>(0, 0);
+    const T rdz = (T)(1.0 / a.dz);
+    C x = mk<T>(0, 0);
+#pragma unroll
+    for (int i = kRegLev - 1; i >= 0; --i) {
+        if (i == ns - 1) {
+            x = mk<T>(y[i].x + vp[i] * xl.x - cp[i] * xr.x, y[i].y + vp[i] * xl.y - cp[i] * xr.y);
+            ph[S * (s + i)] = x;
+        } else if (i < ns - 1) {
+            const C xi = mk<T>(y[i].x + vp[i] * xl.x - cp[i] * x.x, y[i].y + vp[i] * xl.y - cp[i] * x.y);
+            ph[S * (s + i)] = xi;
+            if (dph) dph[S * (s + i + 1)] = mk<T>((x.x - xi.x) * rdz, (x.y - xi.y) * rdz);
+            x = xi;
+        }
+    }
+    if (k > 0) {
+        if (dph) dph[S * s] = mk<T>((x.x - xl.x) * rdz, (x.y - xl.y) * rdz);
+    } else {
+        // Neumann ghost level below the wall (:313-315)
+        const C p0 = mk<T>(x.x - dz * hz0.x, x.y - dz * hz0.y);
+        ph[0] = p0;
+        if (dph) dph[S] = mk<T>((x.x - p0.x) / dz, (x.y - p0.y) / dz);
+    }
+}
+
+bool tdma_reg_supported(int L) { return L >= 1 && L <= kRegSeg * kRegLev; }
+
+template <typename T>
+void launch_tdma_reg(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s, cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    constexpr int bs = 32 * kRegSeg;
+    const int Ls = (a.L + kRegSeg - 1) / kRegSeg, K = (a.L + Ls - 1) / Ls;
+    const int nbi = (int)((isl.n + bs - 1) / bs), nbb = (int)((a.S + 31) / 32);
+    k_tdma_reg<T><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi, Ls, K);
+    e = cudaGetLastError();
+}
+template void launch_tdma_reg<float>(const TdmaArgs<float> &, const IslandArgs &, cudaStream_t, cudaError_t &);
+
 // ----------------------------------------------------------------------------- streaming
 // The level kernels run over (level, x-vector, y) with VW consecutive x per access (2
 // when every pointer is aligned to 2 elements: ldx is even, so a row starts on a

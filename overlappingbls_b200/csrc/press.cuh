@@ -188,6 +188,12 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
 }
 
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e);
+// FP32 bulk columns by the register-segmented partitioned solve (no scratch traffic),
+// FP64 island columns (isl.n may be 0) by the sequential FP64 sweep in the same launch;
+// levels L <= 256
+bool tdma_reg_supported(int L);
+template <typename T> void launch_tdma_reg(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s,
+                                           cudaError_t &e);
 template <typename T> void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl,
                                               cudaStream_t s, cudaError_t &e);
 

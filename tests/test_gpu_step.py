@@ -185,3 +185,43 @@ def test_headline_size_step_is_divergence_free(prec):
     print(f"headline-size step ({prec}): max |div| / max |ddx(u)| = {rel:.2e}")
     assert rel < (1e-11 if prec == "f64" else 2e-4)
     ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "f32"])
+@pytest.mark.parametrize("top", ["neumann", "single"])
+@pytest.mark.parametrize("nx,ny,nzt", [(512, 256, 9), (256, 256, 34), (256, 512, 129), (512, 256, 257)])
+def test_register_segmented_solve(orc, prec, top, nx, ny, nzt):
+    """The FP32 columns' register-segmented partitioned solve (16 segments of up to 16 rows
+    per column, reduced system in shared memory) against the one-sweep solve it replaces and
+    against the oracle: 8 rows (one row per segment), 33 rows (ragged segments), 128 and 256
+    rows; both top modes, with divtz boundary planes; FP64 islands (mixed) or none (f32)."""
+    ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), "mixed")
+    rng = np.random.default_rng(3)
+    pl = identical_inputs({k: np.asfortranarray(0.1 * rng.standard_normal((ctx.ldx, ny))) for k in ("b", "t")},
+                          "mixed")
+    L = ctx.nz - 1
+    outs = {}
+    for reg in (1, 0):
+        ctx.set_param("tdma_reg", reg)
+        u, v, w = (f[k].copy(order="F") for k in "uvw")
+        d, big, p, dp = _alloc_step(ctx)
+        ctx.step(u, v, w, f["theta"], d, big, p, dp, pl["b"], pl["t"])
+        outs[reg] = (p, dp, u, v, w)
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
+    npz = 1 if top == "single" else 2
+    rp, rdx, rdy = g.press_stag_array(f["u"], f["v"], f["w"], pl["b"], pl["t"], npz=npz)
+    rdz = g.dpdz(rp)
+    ru, rv, rw = g.project(f["u"], f["v"], f["w"], rdx, rdy, rdz)
+    # the f32 form has no FP64 islands: its weakly dominant low-|k| columns lose digits
+    # in either solve, so it is held to a loose bound (the mixed form is the checked one)
+    tol = 1e-5 if prec == "mixed" else 1e-2
+    for reg in (1, 0):
+        p, dp, u, v, w = outs[reg]
+        assert rel_l2(p[:nx, :, : L + 1], rp[:nx, :, : L + 1]) < tol, reg
+        for a, r in zip(dp, (rdx, rdy, rdz)):
+            assert rel_l2(a[:nx, :, :L], r[:nx, :, :L]) < tol, reg
+        for a, r in ((u, ru), (v, rv), (w, rw)):
+            assert rel_l2(a, r) < tol, reg
+    # the two FP32 solves agree to FP32 rounding
+    assert rel_l2(outs[1][0][:nx, :, : L + 1], outs[0][0][:nx, :, : L + 1]) < (2e-6 if prec == "mixed" else 5e-3)
