@@ -1988,19 +1988,23 @@ template <typename HT> static int step_host(obl_ctx *ctx, const obl_step_io *io)
     });
 }
 
-// The host step with its copies overlapped (host type = storage type, line-kernel form):
+// The host step with its copies overlapped (line-kernel form):
 //   input stream:   u, v, w, theta host -> device, one event per field;
 //   compute stream: field c's forward kernels as soon as field c has landed, then the
 //                   pressure solve and project();
 //   output stream:  field c's ddx, ddy and padded field device -> host as soon as its
 //                   kernels are done; p, dp*, u, v, w after the solve.
-// The device-to-host volume (about 6 of the 7.6 GB of a 512^2 x 256 step) dominates; it now
-// starts after the first field instead of after the whole step, and the input copies run
-// under it.  Pinned host memory is needed for the copies to overlap; with pageable memory
-// the same calls complete in order.  Results are the same as the staged path.
-template <typename HT> static int step_host_overlapped(obl_ctx *ctx, const obl_step_io *io)
+// The device-to-host volume (about 6 of the 7.6 GB of a 512^2 x 256 FP32 step, 13 of 15 GB
+// with real(8) host arrays) dominates; it now starts after the first field instead of after
+// the whole step, and the input copies run under it.  When the host type HT differs from
+// the storage type T (real(8) arrays of a caller on a mixed-precision context), each input
+// lands in a staging buffer of the host type and is converted on the input stream, and
+// each output is converted on the output stream just before its copy.  Pinned host memory
+// is needed for the copies to overlap; with pageable memory the same calls complete in
+// order.  Results are the same as the staged path.
+template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx, const obl_step_io *io)
 {
-    using T = HT;
+    constexpr bool conv = sizeof(HT) != sizeof(T);
     const long long nf = ctx->field(), nd = ctx->dfield(), nb = ctx->big(), pl = ctx->plane(), ny = ctx->nyt;
     const long long L = ctx->L, nlev = ctx->nz + 1;
     if (cudaSetDevice(ctx->dev) != cudaSuccess) return fail(ctx, OBL_ERR_CUDA, "cudaSetDevice");
@@ -2015,12 +2019,19 @@ template <typename HT> static int step_host_overlapped(obl_ctx *ctx, const obl_s
                          io->d[6], io->d[7], io->big[0], io->big[1], io->big[2], io->big[3], io->p, io->dp[0], io->dp[1],
                          io->dp[2], io->divtz_bot, io->divtz_top};
     if (ctx->stage.size() < 22) ctx->stage.resize(22);
-    void *d[22] = {};
+    if (ctx->stage64.size() < 22) ctx->stage64.resize(22);
+    void *d[22] = {}, *l[22] = {};
     int rc;
     for (int i = 0; i < 22; ++i) {
         if (!h[i]) continue;
         if ((rc = ensure(ctx, ctx->stage[i], sizeof(T) * n[i]))) return rc;
         d[i] = ctx->stage[i].p;
+        if (conv) {
+            if ((rc = ensure(ctx, ctx->stage64[i], sizeof(HT) * n[i]))) return rc;
+            l[i] = ctx->stage64[i].p;
+        } else {
+            l[i] = d[i];
+        }
     }
     obl_step_io dio{};
     dio.u = d[0]; dio.v = d[1]; dio.w = d[2]; dio.theta = d[3];
@@ -2031,13 +2042,30 @@ template <typename HT> static int step_host_overlapped(obl_ctx *ctx, const obl_s
     dio.divtz_bot = d[20];
     dio.divtz_top = d[21];
     const cudaStream_t s = ctx->stream, ci = ctx->cin, co = ctx->cout;
-    auto in = [&](int i) { return cudaMemcpyAsync(d[i], h[i], sizeof(T) * n[i], cudaMemcpyHostToDevice, ci); };
+    // host type -> storage type (or storage -> host) of n elements on stream st
+    auto convert = [&](void *dst, const void *src, long long cnt, bool to_storage, cudaStream_t st) -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        LaunchScope ls(ctx->rec, "convert", st);
+        const bool d2f = to_storage ? (sizeof(HT) == 8) : (sizeof(T) == 8);
+        if (d2f) launch_convert_d2f((float *)dst, (const double *)src, cnt, st, e);
+        else launch_convert_f2d((double *)dst, (const float *)src, cnt, st, e);
+        return e;
+    };
+    auto in = [&](int i) -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(l[i], h[i], sizeof(HT) * n[i], cudaMemcpyHostToDevice, ci);
+        if (e == cudaSuccess && conv) e = convert(d[i], l[i], n[i], true, ci);
+        return e;
+    };
     // rows [row0, row0+nrows) of pitch ld, the first width elements of each (x < nxt)
     auto out = [&](int i, long long ld, long long width, long long row0, long long nrows) -> cudaError_t {
-        char *hd = (char *)h[i] + sizeof(T) * row0 * ld;
-        const char *dd = (const char *)d[i] + sizeof(T) * row0 * ld;
-        if (width == ld) return cudaMemcpyAsync(hd, dd, sizeof(T) * ld * nrows, cudaMemcpyDeviceToHost, co);
-        return cudaMemcpy2DAsync(hd, sizeof(T) * ld, dd, sizeof(T) * ld, sizeof(T) * width, nrows,
+        if (conv) {
+            cudaError_t e = convert((HT *)l[i] + row0 * ld, (const T *)d[i] + row0 * ld, ld * nrows, false, co);
+            if (e != cudaSuccess) return e;
+        }
+        char *hd = (char *)h[i] + sizeof(HT) * row0 * ld;
+        const char *dd = (const char *)l[i] + sizeof(HT) * row0 * ld;
+        if (width == ld) return cudaMemcpyAsync(hd, dd, sizeof(HT) * ld * nrows, cudaMemcpyDeviceToHost, co);
+        return cudaMemcpy2DAsync(hd, sizeof(HT) * ld, dd, sizeof(HT) * ld, sizeof(HT) * width, nrows,
                                  cudaMemcpyDeviceToHost, co);
     };
     if (h[20]) CK(in(20));
@@ -2072,7 +2100,8 @@ template <typename HT> static int step_host_overlapped(obl_ctx *ctx, const obl_s
 
 template <typename HT> static int step_host_any(obl_ctx *ctx, const obl_step_io *io)
 {
-    if (sizeof(HT) == ctx->es() && ctx->param_fused == 0) return step_host_overlapped<HT>(ctx, io);
+    if (ctx->param_fused == 0)
+        return ctx->es() == 4 ? step_host_overlapped<HT, float>(ctx, io) : step_host_overlapped<HT, double>(ctx, io);
     return step_host<HT>(ctx, io);
 }
 

@@ -551,7 +551,13 @@ template <typename T, int N, int OP> constexpr int col_lines()
 }
 // Minimum resident CTAs per SM the column kernels are compiled for: with twiddles through
 // L1, registers are bounded so that the CTAs of 32 warps in total fit on an SM.
-constexpr int col_min_blocks(int nw, bool twg) { return twg ? (nw >= 32 ? 1 : 32 / nw) : 1; }
+#ifndef OBL_COL_WARPS_SM
+#define OBL_COL_WARPS_SM 32   // resident warps per SM the register bound is set for
+#endif
+constexpr int col_min_blocks(int nw, bool twg)
+{
+    return twg ? (nw >= OBL_COL_WARPS_SM ? 1 : OBL_COL_WARPS_SM / nw) : 1;
+}
 
 template <typename T, int N, int OP, int NW = 8, int WB = LmGeo<T>::WB> struct ColDerived {
     using D = LineDerived<N, OP>;
@@ -573,9 +579,13 @@ struct NoColEpi {
 // One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
 // tables twF/twB are already in shared memory; buf is the exchange scratch (NM*WB).
 // Called by k_cols2 (one unit per CTA) and by the persistent ensemble kernel.
-template <typename T, int N, int OP, bool REAL, int NW = 8, int WB_ = LmGeo<T>::WB, class EPI = NoColEpi>
+// tile (SMEM_IN): the unit's input already in shared memory, row i of line l at
+// tile[i*WB + l] (the persistent pipelined kernel below); otherwise read from global.
+template <typename T, int N, int OP, bool REAL, int NW = 8, int WB_ = LmGeo<T>::WB, class EPI = NoColEpi,
+          bool SMEM_IN = false>
 __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, const C2<T> *twF,
-                                           const C2<T> *twB, C2<T> *buf, const EPI &epi = EPI())
+                                           const C2<T> *twB, C2<T> *buf, const EPI &epi = EPI(),
+                                           const C2<T> *tile = nullptr)
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
@@ -594,7 +604,8 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
     const E *srcz = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane;
     E *dstz = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane;
     auto gld = [&](int i) -> C {
-        if constexpr (REAL) return __ldcg(reinterpret_cast<const C *>(srcz + (long long)i * a.src_row + 2 * glc));
+        if constexpr (SMEM_IN) return tile[i * WB + line];
+        else if constexpr (REAL) return __ldcg(reinterpret_cast<const C *>(srcz + (long long)i * a.src_row + 2 * glc));
         else return __ldcg(srcz + (long long)i * a.src_row + glc);
     };
     auto gst = [&](int i, C v) {
@@ -625,7 +636,7 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
 #if OBL_COL_PF
         // the CTA that processes this line group pf_ahead planes later (about one
         // residency window of CTAs) finds its input in L2
-        if (a.pf_ahead > 0 && act && z + a.pf_ahead < a.nlev) {
+        if (!SMEM_IN && a.pf_ahead > 0 && act && z + a.pf_ahead < a.nlev) {
             const E *pz = srcz + (long long)a.pf_ahead * a.src_plane;
 #pragma unroll
             for (int b = 0; b < GG::PER; ++b) {
@@ -745,6 +756,70 @@ __global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG)) k_cols2(ColA
     }
 }
 
+// ----------------------------------------------------------------------------- pipelined columns
+// Persistent form of k_cols2: each CTA walks units u = blockIdx.x, + gridDim.x, ... (line
+// group u % nbx of plane u / nbx) and, while it transforms unit u, the next unit's input
+// tile (NI rows x WB lines) is already on its way into shared memory with 8-byte cp.async
+// copies (every address of a field row is 8-byte aligned; its 2056-byte pitch at nxt = 512
+// is not the 16-byte multiple a tensor map needs).  Two tiles alternate; the exchange
+// scratch is separate.  The loads of the column kernel then no longer stall its warps.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 8 : 0;   // 0: the 8 bytes are zero-filled
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+template <typename T, int N, int OP, bool REAL, int NW, int WB>
+__device__ __forceinline__ void cols_tile_issue(const ColArgs<T> &a, int nbx, int u, C2<T> *tile)
+{
+    using C = C2<T>;
+    using E = typename std::conditional<REAL, T, C>::type;
+    constexpr int NI = LineDerived<N, OP>::NI;
+    const int bx = u % nbx, z = u / nbx;
+    const int nlines = REAL ? a.ncols / 2 : a.ncols;
+    const E *srcz = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane;
+    for (int idx = threadIdx.x; idx < NI * WB; idx += 32 * NW) {
+        const int i = idx / WB, l = idx % WB, gl = bx * WB + l;
+        const bool ok = gl < nlines;
+        const E *g = srcz + (long long)i * a.src_row + (REAL ? 2 * (ok ? gl : 0) : (ok ? gl : 0));
+        cp_async8(tile + idx, g, ok);
+    }
+}
+
+template <typename T, int N, int OP, bool REAL, int NW, int WB>
+__global__ void __launch_bounds__(32 * NW, 2) k_cols2_pipe(ColArgs<T> a, int nbx)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *tile0 = reinterpret_cast<C *>(smraw);
+    C *tile1 = tile0 + D::NI * WB;
+    C *buf = tile1 + D::NI * WB;
+    const int nunits = nbx * a.nlev;
+    int u = blockIdx.x;
+    if (u >= nunits) return;
+    cols_tile_issue<T, N, OP, REAL, NW, WB>(a, nbx, u, tile0);
+    cp_async_commit();
+    for (int it = 0; u < nunits; ++it, u += gridDim.x) {
+        C *cur = (it & 1) ? tile1 : tile0;
+        C *nxt = (it & 1) ? tile0 : tile1;
+        const int un = u + gridDim.x;
+        if (un < nunits) cols_tile_issue<T, N, OP, REAL, NW, WB>(a, nbx, un, nxt);
+        cp_async_commit();
+        cp_async_wait_prev();
+        __syncthreads();
+        cols2_unit<T, N, OP, REAL, NW, WB, NoColEpi, true>(a, u % nbx, u / nbx, a.twF, a.twB, buf, NoColEpi(), cur);
+        __syncthreads();
+    }
+}
+
+#ifndef OBL_COL_PIPE
+#define OBL_COL_PIPE 0   // FP32 y-pad, ddy and y-transform of long lines: persistent prefetching form
+#endif
+
 // ----------------------------------------------------------------------------- launchers
 template <typename T, int N, int OP> inline size_t rows_smem()
 {
@@ -813,6 +888,28 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
     }
     ColArgs<T> a = a0;
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
+    if constexpr (OBL_COL_PIPE && TWG && OP != OP_INV) {
+        static int pres[kMaxDevices] = {};
+        auto pk = k_cols2_pipe<T, N, OP, REAL, NW, WB>;
+        const size_t psm = sizeof(C2<T>) * ((size_t)2 * D::NI * WB + (size_t)D::NM * WB);
+        int pr = ds >= 0 ? pres[ds] : 0;
+        if (!pr) {
+            cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm);
+            if (e != cudaSuccess) return e;
+            int dev = 0, nsm = 0, per = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pk, 32 * NW, psm);
+            pr = nsm * (per > 0 ? per : 1);
+            if (ds >= 0) pres[ds] = pr;
+        }
+        const int nbx = (nlines + WB - 1) / WB;
+        const long long nunits = (long long)nbx * a.nlev;
+        if (nunits < 1) return cudaSuccess;
+        const int grid = (int)(nunits < pr ? nunits : pr);
+        pk<<<grid, 32 * NW, psm, s>>>(a, nbx);
+        return cudaGetLastError();
+    }
     dim3 grid((nlines + WB - 1) / WB, a.nlev);
     // y-pad only: measured 5% faster at 512x512x256; ddy and the y-transform did not gain
     if (OBL_COL_PF && OP == OP_PAD) a.pf_ahead = (int)((OBL_COL_PF * (long long)resident + 4LL * grid.x - 1) / (4LL * grid.x));

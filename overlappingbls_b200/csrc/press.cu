@@ -127,29 +127,30 @@ __global__ void __launch_bounds__(32 * kRegSeg, 1) k_tdma_reg(TdmaArgs<T> a, Isl
     T cp[kRegLev], vp[kRegLev];
     C hz0 = mk<T>(0, 0);
     if (act && ns > 0) {
-        // right-hand sides of rows s..s+ns-1, all loads independent (:203-225)
-        if (k == 0) hz0 = a.Hz[q];   // RHS_col(0) = H_z(0) (:209)
-        C hz[kRegLev + 1];
+        // right-hand sides of rows s..s+ns-1 (:203-225).  Every load is issued without a
+        // condition (levels past the segment clamp to level L+1 and are not used), so all
+        // of the segment's loads are in flight together.
+        const long long qc = q;
+        hz0 = a.Hz[qc];   // RHS_col(0) = H_z(0) (:209), used by segment 0
+        C hz[kRegLev + 1], hx[kRegLev], hy[kRegLev];
 #pragma unroll
-        for (int i = 0; i <= kRegLev; ++i)
-            if (i <= ns) hz[i] = a.Hz[q + S * (s + i)];
+        for (int i = 0; i <= kRegLev; ++i) hz[i] = __ldcs(a.Hz + qc + S * min(s + i, L + 1));
 #pragma unroll
         for (int i = 0; i < kRegLev; ++i) {
-            if (i < ns) {
-                const int iz = s + i;
-                C r;
-                if (!m00) {
-                    const C hx = a.Hx[q + S * iz], hy = a.Hy[q + S * iz];
-                    const C sxy = mk<T>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
-                    C dh = csub(hz[i + 1], hz[i]);
-                    if (iz == 1) dh = cadd(dh, hz0);
-                    r = mk<T>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
-                } else {
-                    r = (iz == 1) ? mk<T>(0, 0) : hz[i];
-                }
-                if (iz == L && !top_solved) r = mk<T>(0, 0);
-                y[i] = r;
-            }
+            const long long zz = min(s + i, L);
+            hx[i] = __ldcs(a.Hx + qc + S * zz);
+            hy[i] = __ldcs(a.Hy + qc + S * zz);
+        }
+#pragma unroll
+        for (int i = 0; i < kRegLev; ++i) {
+            const int iz = s + i;
+            const C sxy = mk<T>(kx * hx[i].x + ky * hy[i].x, kx * hx[i].y + ky * hy[i].y);
+            C dh = csub(hz[i + 1], hz[i]);
+            if (iz == 1) dh = cadd(dh, hz0);
+            C r = mk<T>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+            if (m00) r = (iz == 1) ? mk<T>(0, 0) : hz[i];
+            if (iz == L && !top_solved) r = mk<T>(0, 0);
+            y[i] = r;
         }
         // forward sweep with x_{s-1} left unknown: x_i = y'_i + v'_i x_{s-1} - c'_i x_{i+1}
         T cprev = 0, vprev = 1;

@@ -209,7 +209,7 @@ def test_register_segmented_solve(orc, prec, top, nx, ny, nzt):
         ctx.step(u, v, w, f["theta"], d, big, p, dp, pl["b"], pl["t"])
         outs[reg] = (p, dp, u, v, w)
     g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
-    npz = 1 if top == "single" else 2
+    npz = 1 if top == "single" else (2 if L % 2 == 0 else 3)   # the oracle's ranks need whole levels
     rp, rdx, rdy = g.press_stag_array(f["u"], f["v"], f["w"], pl["b"], pl["t"], npz=npz)
     rdz = g.dpdz(rp)
     ru, rv, rw = g.project(f["u"], f["v"], f["w"], rdx, rdy, rdz)
