@@ -1,5 +1,5 @@
 // fft.cuh -- complex arithmetic helpers and the in-register DFT codelets (radix 2, 3,
-// 4 and the composites 6, 8, 9, 12, 16) used by the Stockham passes of fft2.cuh.
+// 4, 5 and the composites 6, 8, 9, 10, 12, 16) used by the Stockham passes of fft2.cuh.
 //
 // Convention (FFTW's, which the reference relies on, SBL/code/002_fft.f90:97-113):
 //   forward  X[k] = sum_j x[j] exp(-2 pi i j k / N)
@@ -187,6 +187,35 @@ template <bool FWD> struct Dft<4, FWD> {
     }
 };
 
+// 5-point DFT from its two conjugate-symmetric pairs (x1, x4) and (x2, x3):
+//   X_k = x0 + c_k (x1 + x4) + c_2k (x2 + x3) -+ i [s_k (x1 - x4) + s_2k (x2 - x3)],
+// with c_k = cos(2 pi k/5), s_k = sin(2 pi k/5); the sign is - for forward.
+template <bool FWD> struct Dft<5, FWD> {
+    template <typename C> __device__ __forceinline__ static void run(C *x)
+    {
+        using T = decltype(x[0].x);
+        const T c1 = (T)ct::cos2pi(1, 5), c2 = (T)ct::cos2pi(2, 5);
+        const T s1 = (T)ct::cos2pi(4 * 1 - 5, 20), s2 = (T)ct::cos2pi(4 * 2 - 5, 20);
+        const C t1 = cadd(x[1], x[4]), t2 = cadd(x[2], x[3]);
+        const C t3 = csub(x[1], x[4]), t4 = csub(x[2], x[3]);
+        C a1, a2, b1, b2;
+        a1.x = x[0].x + c1 * t1.x + c2 * t2.x;
+        a1.y = x[0].y + c1 * t1.y + c2 * t2.y;
+        a2.x = x[0].x + c2 * t1.x + c1 * t2.x;
+        a2.y = x[0].y + c2 * t1.y + c1 * t2.y;
+        b1.x = s1 * t3.x + s2 * t4.x;
+        b1.y = s1 * t3.y + s2 * t4.y;
+        b2.x = s2 * t3.x - s1 * t4.x;
+        b2.y = s2 * t3.y - s1 * t4.y;
+        const C m1 = mul_mi<FWD>(b1), m2 = mul_mi<FWD>(b2);
+        x[0] = cadd(x[0], cadd(t1, t2));
+        x[1] = cadd(a1, m1);
+        x[4] = csub(a1, m1);
+        x[2] = cadd(a2, m2);
+        x[3] = csub(a2, m2);
+    }
+};
+
 // Composite codelet R = A*B (four-step, all indices compile time):
 //   X[q + B p] = sum_l w_A^{lp} w_R^{lq} sum_m x[l + A m] w_B^{mq}
 template <int A, int B, bool FWD> struct DftComp {
@@ -219,5 +248,6 @@ template <bool FWD> struct Dft<8, FWD> : DftComp<2, 4, FWD> {};
 template <bool FWD> struct Dft<9, FWD> : DftComp<3, 3, FWD> {};
 template <bool FWD> struct Dft<12, FWD> : DftComp<4, 3, FWD> {};
 template <bool FWD> struct Dft<16, FWD> : DftComp<4, 4, FWD> {};
+template <bool FWD> struct Dft<10, FWD> : DftComp<2, 5, FWD> {};
 
 } // namespace obl

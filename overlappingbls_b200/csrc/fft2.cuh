@@ -54,6 +54,13 @@ template <> struct Base<192> { using type = RPlan<4, 6, 8>; };
 template <> struct Base<256> { using type = RPlan<4, 8, 8>; };
 template <> struct Base<384> { using type = RPlan<6, 8, 8>; };
 template <> struct Base<512> { using type = RPlan<8, 8, 8>; };
+// lengths with a factor 5 (FFTW plans any length, 002_fft.f90:78-117); the middle radix
+// carries the 5 so that the last one stays even for its 3/2-rule partner
+template <> struct Base<80> { using type = RPlan<4, 5, 4>; };
+template <> struct Base<160> { using type = RPlan<4, 5, 8>; };
+template <> struct Base<240> { using type = RPlan<6, 5, 8>; };
+template <> struct Base<320> { using type = RPlan<8, 5, 8>; };
+template <> struct Base<640> { using type = RPlan<8, 10, 8>; };
 
 template <class P> struct PadOf;
 template <int R0, int R1, int R2> struct PadOf<RPlan<R0, R1, R2>> { using type = RPlan<R0, R1, 3 * R2 / 2>; };

@@ -7,7 +7,8 @@
 
 #include "lines.cuh"
 
-#define OBL_FOR_EACH_N(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+#define OBL_FOR_EACH_N(X) \
+    X(32) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(240) X(256) X(320) X(384) X(512) X(640)
 
 namespace obl {
 

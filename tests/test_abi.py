@@ -46,6 +46,23 @@ def test_bad_grid_rejected_before_touching_the_gpu():
     assert not h.value
 
 
+@pytest.mark.parametrize("n,ok", [(80, True), (160, True), (240, True), (320, True), (640, True),
+                                  (512, True), (72, False), (100, False), (1024, False)])
+def test_line_lengths_with_plans(n, ok):
+    """Lengths with a compiled plan (radix 2, 3, 4, 5 chains and their 3/2 partners) pass the
+    length check, which runs before any device call; others give OBL_ERR_UNSUPPORTED."""
+    lib = obl.load_library()
+    h = ctypes.c_void_p()
+    g = obl.Grid(n, 64, 9, 1.0, 1.0, 1.0, 1.0, 0.1, 1.0)
+    rc = lib.obl_ctx_create(ctypes.byref(g), None, ctypes.byref(h))
+    if ok:
+        assert rc != 5
+        if rc == 0:
+            lib.obl_ctx_destroy(h)
+    else:
+        assert rc == 5
+
+
 @pytest.mark.skipif(gpu_present(), reason="checks the no-device path")
 def test_no_device_fails_loudly():
     with pytest.raises(obl.OblError, match="NODEV"):

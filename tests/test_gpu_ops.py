@@ -15,6 +15,9 @@ GRIDS = {
     "config0": (64, 64, 65),      # the reference's CPU-runnable case
     "rect": (96, 64, 33),         # nx != ny, radix-3 lengths
     "rect2": (128, 192, 17),
+    "radix5": (80, 160, 17),      # lengths with a factor 5 (and their 3/2 partners 120, 240)
+    "radix5b": (320, 240, 9),
+    "radix5c": (640, 80, 5),
 }
 
 

@@ -225,3 +225,27 @@ def test_register_segmented_solve(orc, prec, top, nx, ny, nzt):
             assert rel_l2(a, r) < tol, reg
     # the two FP32 solves agree to FP32 rounding
     assert rel_l2(outs[1][0][:nx, :, : L + 1], outs[0][0][:nx, :, : L + 1]) < (2e-6 if prec == "mixed" else 5e-3)
+
+
+@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("nx,ny,nzt", [(80, 160, 17), (320, 240, 9), (640, 640, 5)])
+def test_step_factor5_lengths(orc, prec, nx, ny, nzt):
+    """The fused step on grids whose lengths have a factor 5 (radix-5 and radix-10 plans,
+    3/2 partners 120 ... 960) against the oracle, every output."""
+    ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc="neumann", **fields.DOMAIN)
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
+    u, v, w = (f[k].copy(order="F") for k in "uvw")
+    d, big, p, dp = _alloc_step(ctx)
+    ctx.step(u, v, w, f["theta"], d, big, p, dp)
+    ref = g.step(f["u"], f["v"], f["w"], f["theta"], npz=2)
+    L = g.nz - 1
+    for i in range(8):
+        assert rel_l2(d[i][:nx], ref["d"][i][:nx]) < TOL[prec], i
+    for i in range(4):
+        assert rel_l2(big[i], ref["big"][i]) < TOL[prec], i
+    assert rel_l2(p[:nx, :, : L + 1], ref["p"][:nx, :, : L + 1]) < TOL[prec]
+    for a, k in zip(dp, ("dpdx", "dpdy", "dpdz")):
+        assert rel_l2(a[:nx, :, :L], ref[k][:nx, :, :L]) < TOL[prec], k
+    for a, k in ((u, "u"), (v, "v"), (w, "w")):
+        assert rel_l2(a, ref[k]) < TOL[prec], k
