@@ -211,10 +211,11 @@ def algorithmic_bytes(name, info, s):
         # one launch per field: field in, ddx and the x-padded rows out, and on u, v, w the
         # RHS x-spectrum of levels 1..L out (mean over the 4 launches of a step)
         "rows_fwd3": ((2 * nx + nx2) * ny * nlev * s * 4 + 3 * lhx * ny * L * c) / 4,
-        # p_hat (0..L) and the dpdz spectrum in; y-inverses of p, dpdx, dpdy, dpdz out
-        "pinv_cols": (2 * L + 1) * lhx * ny * c + (4 * L + 1) * lhx * ny * c,
-        # the four y-inverses and u, v, w in; p, dpdx, dpdy, dpdz and u, v, w out
-        "pinv_rows_project": (4 * L + 1) * lhx * ny * c + 3 * nx * ny * L * s + (4 * L + 1) * nx * ny * s
+        # p_hat (0..L) and the dpdz spectrum in; y-inverses of p, dpdy, dpdz out (dpdx's is
+        # i*kx times that of p, formed by the row pass)
+        "pinv_cols": (2 * L + 1) * lhx * ny * c + (3 * L + 1) * lhx * ny * c,
+        # the three y-inverses and u, v, w in; p, dpdx, dpdy, dpdz and u, v, w out
+        "pinv_rows_project": (3 * L + 1) * lhx * ny * c + 3 * nx * ny * L * s + (4 * L + 1) * nx * ny * s
                              + 3 * nx * ny * L * s,
     }
     return table.get(name)

@@ -507,7 +507,7 @@ template <typename T> struct Ops {
             // one x-inverse pass over the rows that also applies project()
             PinvColArgs<T> pc{};
             pc.ph = ph; pc.dph = (const C2<T> *)ctx->spec[4].p;
-            pc.Xp = Hz; pc.Xdx = Hx; pc.Xdy = Hy; pc.Xdz = (C2<T> *)ctx->spec[4].p;
+            pc.Xp = Hz; pc.Xdy = Hy; pc.Xdz = (C2<T> *)ctx->spec[4].p;
             pc.S = S; pc.lhx = lhx; pc.kx = ctx->d_kx; pc.ky = ctx->d_ky2;
             pc.twB = twt<T>(ctx, ny, ROLE_BWD);
             {
@@ -515,7 +515,7 @@ template <typename T> struct Ops {
                 if ((rc = chk(PinvLaunch<T>::cols(ny, pc, L + 1, s()), "pinv_cols"))) return rc;
             }
             PinvRowArgs<T> pr{};
-            pr.Xp = Hz; pr.Xdx = Hx; pr.Xdy = Hy; pr.Xdz = (const C2<T> *)ctx->spec[4].p;
+            pr.Xp = Hz; pr.kx = ctx->d_kx; pr.Xdy = Hy; pr.Xdz = (const C2<T> *)ctx->spec[4].p;
             pr.p = p; pr.dpdx = dpdx; pr.dpdy = dpdy; pr.dpdz = dpdz_out;
             pr.u = (T *)proj->u; pr.v = (T *)proj->v; pr.w = (T *)proj->w;
             pr.npairs = (long long)ny * (L + 1) / 2;
@@ -1048,14 +1048,14 @@ template <typename T> struct Ops {
         C2<T> *Hx = (C2<T> *)ctx->spec[0].p, *Hy = (C2<T> *)ctx->spec[1].p, *Hz = (C2<T> *)ctx->spec[2].p;
         C2<T> *ph = (C2<T> *)ctx->spec[3].p, *dph = (C2<T> *)ctx->spec[4].p;
         PinvColArgs<T> pc{};
-        pc.ph = ph; pc.dph = dph; pc.Xp = Hz; pc.Xdx = Hx; pc.Xdy = Hy; pc.Xdz = dph;
+        pc.ph = ph; pc.dph = dph; pc.Xp = Hz; pc.Xdy = Hy; pc.Xdz = dph;
         pc.S = S; pc.lhx = lhx; pc.kx = ctx->d_kx; pc.ky = ctx->d_ky2; pc.twB = twt<T>(ctx, ny, ROLE_BWD);
         {
             LaunchScope ls(ctx->rec, "pinv_cols", s());
             if ((rc = chk(PinvLaunch<T>::cols(ny, pc, L + 1, s()), "pinv_cols"))) return rc;
         }
         PinvRowArgs<T> pr{};
-        pr.Xp = Hz; pr.Xdx = Hx; pr.Xdy = Hy; pr.Xdz = dph;
+        pr.Xp = Hz; pr.kx = ctx->d_kx; pr.Xdy = Hy; pr.Xdz = dph;
         pr.p = (T *)io->p; pr.dpdx = (T *)io->dp[0]; pr.dpdy = (T *)io->dp[1]; pr.dpdz = (T *)io->dp[2];
         pr.u = (T *)io->u; pr.v = (T *)io->v; pr.w = (T *)io->w;
         pr.npairs = (long long)ny * (L + 1) / 2;
@@ -1132,11 +1132,11 @@ template <typename T> struct Ops {
         I.isl_units = (ctx->n_isl + 255) / 256;
         I.bulk_units = (S + 255) / 256;
         PinvColArgs<T> &pc = I.pc;
-        pc.ph = ph; pc.dph = dph; pc.Xp = H[2]; pc.Xdx = H[0]; pc.Xdy = H[1]; pc.Xdz = dph;
+        pc.ph = ph; pc.dph = dph; pc.Xp = H[2]; pc.Xdy = H[1]; pc.Xdz = dph;
         pc.S = S; pc.lhx = lhx; pc.kx = ctx->d_kx; pc.ky = ctx->d_ky2; pc.twB = twt<T>(ctx, ny, ROLE_BWD);
         I.pc_nb = (lhx + WB - 1) / WB;
         PinvRowArgs<T> &pr = I.pr;
-        pr.Xp = H[2]; pr.Xdx = H[0]; pr.Xdy = H[1]; pr.Xdz = dph;
+        pr.Xp = H[2]; pr.kx = ctx->d_kx; pr.Xdy = H[1]; pr.Xdz = dph;
         pr.p = (T *)io->p; pr.dpdx = (T *)io->dp[0]; pr.dpdy = (T *)io->dp[1]; pr.dpdz = (T *)io->dp[2];
         pr.u = (T *)io->u; pr.v = (T *)io->v; pr.w = (T *)io->w;
         pr.npairs = (long long)ny * (L + 1) / 2;

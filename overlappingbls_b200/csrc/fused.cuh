@@ -324,12 +324,13 @@ template <typename T> struct RowsFwd3Launch {
 };
 
 // ----------------------------------------------------------------------------- fused inverse
-// y-inverse of the pressure solution: one load of p_hat(z) gives the y-inverses of p_hat,
-// i*kx*p_hat and i*ky*p_hat (109_press_stag_array.f90:231-238), one load of the dpdz
-// spectrum gives its y-inverse.  Level 0 only needs p.  Line-minor column layout.
+// y-inverse of the pressure solution: one load of p_hat(z) gives the y-inverses of p_hat
+// and i*ky*p_hat (109_press_stag_array.f90:231-238), one load of the dpdz spectrum gives
+// its y-inverse; i*kx*p_hat is formed from the y-inverse of p_hat by the row pass.  Level
+// 0 only needs p.  Line-minor column layout.
 template <typename T> struct PinvColArgs {
     const C2<T> *ph, *dph;                // (lhx, ny, 0..L) spectra
-    C2<T> *Xp, *Xdx, *Xdy, *Xdz;          // y-inverses, same layout
+    C2<T> *Xp, *Xdy, *Xdz;                // y-inverses of p_hat, i*ky*p_hat, dpdz spectrum
     long long S;                          // lhx*ny
     int lhx;
     const double *kx, *ky;                // kx(lhx), ky_2d row (ny)
@@ -383,11 +384,8 @@ __device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, 
     fft_regs<N, typename D::PB, LL, false, true>(w, sc, twB, t);
     store(a.Xp, w);
     if (z == 0) return;   // uniform per block
-    const T kxv = (T)a.kx[glc];
-#pragma unroll
-    for (int q = 0; q < VR; ++q) w[q] = mk<T>(-kxv * v[q].y, kxv * v[q].x);
-    fft_regs<N, typename D::PB, LL, false, true>(w, sc, twB, t);
-    store(a.Xdx, w);
+    // i*kx p_hat needs no transform of its own: kx is constant along y, so its y-inverse
+    // is i*kx times that of p_hat, applied by the x-inverse row pass when it loads Xp
 #pragma unroll
     for (int b = 0; b < G0::PER; ++b) {
         const int j = t + LL * b;
@@ -427,7 +425,8 @@ __global__ void __launch_bounds__(32 * NW, TWG ? 4 : 2) k_cols_pinv(PinvColArgs<
 // pass over the rows: p at levels 0..L, dpdx/dpdy/dpdz at 1..L (slot z-1), and
 // u,v (levels 1..L) and w (levels 2..L) += dt*(-tadv1*grad p).
 template <typename T> struct PinvRowArgs {
-    const C2<T> *Xp, *Xdx, *Xdy, *Xdz;    // (lhx, ny, 0..L)
+    const C2<T> *Xp, *Xdy, *Xdz;          // (lhx, ny, 0..L); dpdx's is i*kx*Xp
+    const double *kx;                     // kx(lhx), Nyquist entry 0
     T *p, *dpdx, *dpdy, *dpdz;            // p (ldx, ny, 0:nz); d* (ldx, ny, 1:nz)
     T *u, *v, *w;                         // updated in place (ldx, ny, 0:nz)
     long long npairs;                     // ny*(L+1)/2
@@ -467,7 +466,7 @@ __device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long lon
         const int z = (int)((2 * base) / a.ny);            // warp-uniform level
         if (q > 0 && z == 0) return;                       // level 0 holds p only
         const long long off = (r0 % a.ny) * a.ldx;
-        const C *X = q == 0 ? a.Xp : q == 1 ? a.Xdx : q == 2 ? a.Xdy : a.Xdz;
+        const C *X = q <= 1 ? a.Xp : q == 2 ? a.Xdy : a.Xdz;
         T *out = q == 0 ? a.p + pl * z + off : (q == 1 ? a.dpdx : q == 2 ? a.dpdy : a.dpdz) + pl * (z - 1) + off;
         T *f = (q == 1 ? a.u : q == 2 ? a.v : a.w) + pl * z + off;
         const bool proj = q == 1 || q == 2 || (q == 3 && z >= (a.w_from_1 ? 1 : 2));   // jz_min for w
@@ -500,6 +499,11 @@ __device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long lon
                         const bool lo = i <= N / 2;
                         const int k = lo ? i : N - i;
                         C av = __ldcg(A + k), bv = __ldcg(B + k);
+                        if (q == 1) {   // dpdx: i*kx times the y-inverse of p_hat
+                            const T kk = (T)a.kx[k];
+                            av = mk<T>(-kk * av.y, kk * av.x);
+                            bv = mk<T>(-kk * bv.y, kk * bv.x);
+                        }
                         if (k == 0 || k == N / 2) { av.y = 0; bv.y = 0; }
                         zz = lo ? mk<T>(av.x - bv.y, av.y + bv.x) : mk<T>(av.x + bv.y, bv.x - av.y);
                     }
