@@ -2360,7 +2360,7 @@ static const EnsPart kEnsSplit[3] = {{0, 1, 2}, {1, 4, 4}, {4, 6, 2}};
 
 template <typename T> static int ens_part_bps(const EnsPart &p, size_t smem)
 {
-    if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, 2>::blocks_per_sm(smem);
+    if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, OBL_ENS_MINB>::blocks_per_sm(smem);
     if (p.pb == 0) return EnsKernel<T, 0, 1, 2>::blocks_per_sm(smem);
     if (p.pb == 1) return EnsKernel<T, 1, 4, 4>::blocks_per_sm(smem);
     return EnsKernel<T, 4, 6, 2>::blocks_per_sm(smem);
@@ -2368,7 +2368,7 @@ template <typename T> static int ens_part_bps(const EnsPart &p, size_t smem)
 template <typename T> static cudaError_t ens_part_launch(const EnsPart &p, const EnsArgs<T> &a, int blocks, size_t smem,
                                                         cudaStream_t s)
 {
-    if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, 2>::launch(a, blocks, smem, s);
+    if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, OBL_ENS_MINB>::launch(a, blocks, smem, s);
     if (p.pb == 0) return EnsKernel<T, 0, 1, 2>::launch(a, blocks, smem, s);
     if (p.pb == 1) return EnsKernel<T, 1, 4, 4>::launch(a, blocks, smem, s);
     return EnsKernel<T, 4, 6, 2>::launch(a, blocks, smem, s);

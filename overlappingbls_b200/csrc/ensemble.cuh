@@ -71,6 +71,9 @@ template <typename T> int ens_wb();   // lines per CTA of the line-minor column 
 // The kernel over phases [PB, PE) with MINB CTAs per SM.  Instantiated: <0,6,2> (the whole
 // step in one launch) and the register-class split <0,1,2> (rows), <1,4,4> (columns, solve,
 // y-inverse), <4,6,2> (x-inverse + project).
+#ifndef OBL_ENS_MINB
+#define OBL_ENS_MINB 2   // CTAs per SM the one-launch persistent kernel's registers are bounded for
+#endif
 template <typename T, int PB, int PE, int MINB> struct EnsKernel {
     static cudaError_t attr(size_t smem);
     static int blocks_per_sm(size_t smem);            // CTAs of the kernel resident per SM

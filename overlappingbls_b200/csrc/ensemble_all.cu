@@ -2,6 +2,6 @@
 #include "ensemble_kernel.cuh"
 
 namespace obl {
-template struct EnsKernel<float, 0, 6, 2>;
-template struct EnsKernel<double, 0, 6, 2>;
+template struct EnsKernel<float, 0, 6, OBL_ENS_MINB>;
+template struct EnsKernel<double, 0, 6, OBL_ENS_MINB>;
 } // namespace obl
