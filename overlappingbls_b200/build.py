@@ -1,6 +1,6 @@
 """Build libobl_b200.so (sm_100a) in-tree with nvcc.
 
-    python -m overlappingbls_b200.build [--force] [-j N] [-D NAME=VALUE ...] [--out PATH]
+    python -m overlappingbls_b200.build [--force] [-j N] [-D NAME=VALUE ...] [--out PATH] [--tuned [WORKLOAD]]
 
 Objects go to overlappingbls_b200/_build/ (git-ignored); the shared library is
 written next to this file so that it travels with the source tree.  -D passes
@@ -81,9 +81,16 @@ if __name__ == "__main__":
     ap.add_argument("-j", type=int, default=None)
     ap.add_argument("-D", dest="defines", action="append", default=[])
     ap.add_argument("--out", default=None)
+    ap.add_argument("--tuned", nargs="?", const="512x512x256", default=None, metavar="WORKLOAD",
+                    help="add the schedule the tuner's cache chose for WORKLOAD (overlappingbls_b200.tune)")
     a = ap.parse_args()
+    defines = list(a.defines)
+    if a.tuned:
+        from overlappingbls_b200 import tune
+        defines += tune.tuned_defines(a.tuned)
+        print("tuned schedule:", defines or "default")
     try:
-        build(force=a.force, jobs=a.j, verbose=True, defines=a.defines, out=a.out)
+        build(force=a.force or bool(a.tuned), jobs=a.j, verbose=True, defines=defines, out=a.out)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

@@ -499,11 +499,6 @@ __device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long lon
                         const bool lo = i <= N / 2;
                         const int k = lo ? i : N - i;
                         C av = __ldcg(A + k), bv = __ldcg(B + k);
-                        if (q == 1) {   // dpdx: i*kx times the y-inverse of p_hat
-                            const T kk = (T)a.kx[k];
-                            av = mk<T>(-kk * av.y, kk * av.x);
-                            bv = mk<T>(-kk * bv.y, kk * bv.x);
-                        }
                         if (k == 0 || k == N / 2) { av.y = 0; bv.y = 0; }
                         zz = lo ? mk<T>(av.x - bv.y, av.y + bv.x) : mk<T>(av.x + bv.y, bv.x - av.y);
                     }
@@ -511,6 +506,10 @@ __device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long lon
                 }
             }
         }
+        // dpdx: i*kx times the y-inverse of p_hat.  On the two Hermitian rows packed as
+        // Z = A + iB that is i*k_signed*Z (k_signed = kx(k) for bins k <= N/2, -kx(N-k)
+        // above), the multiplier of the x-derivative, applied after the loads
+        if (q == 1) reg_deriv<T, N, R0, LL>(v, a.kx, t);
         fft_regs<N, typename D::PB, LL, false>(v, sc, twB, t);
         if (act) {
 #pragma unroll

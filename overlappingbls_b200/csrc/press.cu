@@ -75,12 +75,16 @@ void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_
 // The bands, RHS and boundary rows are those of tdma_column (109_press_stag_array.f90:
 // 4-63, 203-225, 280-317); the rows are the same, only the elimination order differs.
 // FP64 island columns keep the sequential FP64 sweep, in the launch's first nbi blocks.
-constexpr int kRegSeg = 16;   // warps per CTA = segments per column
-constexpr int kRegLev = 16;   // rows a segment keeps in registers (so L <= 256)
+constexpr int kRegSegMax = 16;   // warps per CTA = segments per column, at most
+constexpr int kRegLev = 16;      // rows a segment keeps in registers (so L <= 256)
 
-template <typename T>
-__global__ void __launch_bounds__(32 * kRegSeg, 1) k_tdma_reg(TdmaArgs<T> a, IslandArgs isl, int nbi, int Ls, int K)
+// NSEG segments (warps) per column; 16 / NSEG CTAs per SM, so fewer levels run with
+// smaller CTAs that overlap one another's load, solve and store phases
+template <typename T, int NSEG>
+__global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaArgs<T> a, IslandArgs isl, int nbi,
+                                                                          int Ls, int K)
 {
+    constexpr int kRegSeg = NSEG;
     using C = C2<T>;
     if ((int)blockIdx.x < nbi) {
         tdma_column<T, double, true>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
@@ -262,17 +266,27 @@ __global__ void __launch_bounds__(32 * kRegSeg, 1) k_tdma_reg(TdmaArgs<T> a, Isl
     }
 }
 
-bool tdma_reg_supported(int L) { return L >= 1 && L <= kRegSeg * kRegLev; }
+bool tdma_reg_supported(int L) { return L >= 1 && L <= kRegSegMax * kRegLev; }
+
+template <typename T, int NSEG>
+static void launch_tdma_reg_n(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s, cudaError_t &e)
+{
+    constexpr int bs = 32 * NSEG;
+    const int Ls = (a.L + NSEG - 1) / NSEG, K = (a.L + Ls - 1) / Ls;
+    const int nbi = (int)((isl.n + bs - 1) / bs), nbb = (int)((a.S + 31) / 32);
+    k_tdma_reg<T, NSEG><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi, Ls, K);
+    e = cudaGetLastError();
+}
 
 template <typename T>
 void launch_tdma_reg(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s, cudaError_t &e)
 {
     if (e != cudaSuccess) return;
-    constexpr int bs = 32 * kRegSeg;
-    const int Ls = (a.L + kRegSeg - 1) / kRegSeg, K = (a.L + Ls - 1) / Ls;
-    const int nbi = (int)((isl.n + bs - 1) / bs), nbb = (int)((a.S + 31) / 32);
-    k_tdma_reg<T><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi, Ls, K);
-    e = cudaGetLastError();
+    // the fewest segments that keep every segment within kRegLev rows
+    if (a.L > 8 * kRegLev) launch_tdma_reg_n<T, 16>(a, isl, s, e);
+    else if (a.L > 4 * kRegLev) launch_tdma_reg_n<T, 8>(a, isl, s, e);
+    else if (a.L > 2 * kRegLev) launch_tdma_reg_n<T, 4>(a, isl, s, e);
+    else launch_tdma_reg_n<T, 2>(a, isl, s, e);
 }
 template void launch_tdma_reg<float>(const TdmaArgs<float> &, const IslandArgs &, cudaStream_t, cudaError_t &);
 

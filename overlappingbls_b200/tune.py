@@ -1,6 +1,6 @@
 """Autotuner of the step's execution choices, cached per device in a JSON file.
 
-Two kinds of entries:
+Three kinds of entries:
 
 * ``step``: per (nxt, nyt, nzt, precision) the single-instance step variant: ``fused``
   0 (multi-output line kernels), 1 (cluster-fused forward plane kernel, square grids; with
@@ -9,6 +9,16 @@ Two kinds of entries:
   precision) the ensemble mode (sequential, concurrent streams, one persistent launch,
   the register-class split of it), whether to replay a CUDA graph, and the persistent
   kernel's CTAs per SM.
+* ``build``: per bench workload the compile-time schedule of the kernels: CTA shapes of
+  the column FFT kernels (warps and lines per CTA, resident warps per SM), the persistent
+  prefetching column form, the y-pad's L2 look-ahead, the scratch padding of the row FFT
+  kernels.
+  Each candidate is a set of -D definitions; ``build_variants`` compiles one library per
+  candidate, ``tune_build`` times each through ``bench.py`` (a subprocess with $OBL_LIB),
+  and ``python -m overlappingbls_b200.build --tuned`` compiles the chosen schedule.
+
+The step entries also search the pressure solve's schedule (register-segmented or one
+sweep per column; column segments) next to the forward-pass variant.
 
 Each candidate is timed with CUDA events over ``reps`` steps after ``warmup`` steps; the
 fastest wins.  Results do not depend on any of these choices (the tests check every
@@ -71,13 +81,97 @@ def ensemble_key(shapes, precision):
 
 
 def step_candidates(nxt, nyt):
-    """The variants of the single-instance step worth timing for this grid."""
-    cands = [{"fused": 0}, {"fused": 2}]
+    """The variants of the single-instance step worth timing for this grid: the forward
+    pass (multi-output line kernels, one kernel per routine, cluster-fused planes) and,
+    with the line kernels, the pressure solve's schedule."""
+    cands = [{"fused": 0, "tdma_reg": 1, "tdma_segments": 0}, {"fused": 0, "tdma_reg": 0, "tdma_segments": 0},
+             {"fused": 0, "tdma_reg": 1, "tdma_segments": 4}, {"fused": 0, "tdma_reg": 1, "tdma_segments": 16},
+             {"fused": 2}]
     if nxt == nyt:
         for csize in (4, 8):
             for ncl in (0, 16):
                 cands.append({"fused": 1, "fwd_cluster_size": csize, "fwd_clusters": ncl})
     return cands
+
+
+# Compile-time schedules searched by tune_build (name -> -D definitions).  "default" is the
+# library as built without definitions.
+BUILD_CANDIDATES = {
+    "default": [],
+    "cols_4w4l": ["OBL_PAD_NW=4", "OBL_PAD_WB=4", "OBL_COLS_NW=4", "OBL_COLS_WB=4"],
+    "cols_16w_32sm": ["OBL_PAD_NW=16", "OBL_COLS_NW=16"],
+    "cols_16w_48sm": ["OBL_PAD_NW=16", "OBL_COLS_NW=16", "OBL_COL_WARPS_SM=48"],
+    "cols_pipelined": ["OBL_COL_PIPE=1"],
+    "rows_pad16": ["OBL_SIDX_SHIFT=4"],
+    "pad_prefetch_off": ["OBL_COL_PF=0"],
+}
+
+
+def variant_path(out_dir, name):
+    return os.path.join(out_dir, f"libobl_{name}.so")
+
+
+def build_variants(out_dir, names=None, jobs=None):
+    """Compile one library per build candidate into out_dir (skips existing ones)."""
+    from . import build as b
+    os.makedirs(out_dir, exist_ok=True)
+    done = {}
+    for name in names or BUILD_CANDIDATES:
+        if name == "default":   # timed with the library as built
+            continue
+        lib = variant_path(out_dir, name)
+        if not os.path.exists(lib):
+            b.build(jobs=jobs, defines=BUILD_CANDIDATES[name], out=lib)
+        done[name] = lib
+    return done
+
+
+def bench_ms(lib, workload, steps, warmup, timeout=900):
+    """ms per step of bench.py's step on workload with library lib (None: the default)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ)
+    if lib:
+        env["OBL_LIB"] = os.path.abspath(lib)
+    cmd = [sys.executable, os.path.join(root, "bench.py"), "--workload", workload, "--steps", str(steps),
+           "--warmup", str(warmup), "--skip-fp64", "--skip-e2e", "--skip-cpu"]
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
+    if r.returncode != 0:
+        return None
+    for line in r.stdout.splitlines():
+        if line.startswith("{"):
+            return float(json.loads(line)["ms_per_step"])
+    return None
+
+
+def tune_build(workload, out_dir, names=None, steps=20, warmup=5, path=None, device=None):
+    """Time every built variant on workload, cache all timings and the fastest schedule
+    under ``build``/workload.  Returns (name, defines, ms)."""
+    device = device or _device_name()
+    timings = []
+    for name in names or BUILD_CANDIDATES:
+        lib = variant_path(out_dir, name) if name != "default" else None
+        if lib and not os.path.exists(lib):
+            timings.append(({"name": name, "defines": BUILD_CANDIDATES[name]}, None))
+            continue
+        timings.append(({"name": name, "defines": BUILD_CANDIDATES[name]}, bench_ms(lib, workload, steps, warmup)))
+    best, ms = pick(timings)
+    cache = load_cache(path)
+    ent = _entry(cache, device, "build")
+    ent[workload] = {"params": best, "ms": ms, "timings": [[p, t] for p, t in timings]}
+    save_cache(cache, path)
+    return best["name"], best["defines"], ms
+
+
+def tuned_defines(workload="512x512x256", path=None, device=None):
+    """The -D definitions of the cached fastest schedule for workload ([] if none)."""
+    cache = load_cache(path)
+    devs = cache.get("devices", {})
+    if device is None:
+        device = next((d for d in devs if workload in devs[d].get("build", {})), None)
+    ent = devs.get(device, {}).get("build", {}).get(workload)
+    return list(ent["params"]["defines"]) if ent else []
 
 
 ENSEMBLE_CANDIDATES = (
@@ -180,3 +274,31 @@ def tune_ensemble(ens, ios, shapes, path=None, warmup=3, reps=10, retune=False):
     ent[key] = {"params": best, "ms": ms, "timings": [[p, t] for p, t in timings]}
     save_cache(cache, path)
     return best, ms
+
+
+def main():
+    import argparse
+    ap = argparse.ArgumentParser(description="compile-time schedule sweep of the step's kernels")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    b = sub.add_parser("build-variants", help="compile one library per schedule candidate")
+    b.add_argument("--out", required=True)
+    b.add_argument("--only", nargs="*")
+    t = sub.add_parser("sweep", help="time the built variants on a workload and cache the choice")
+    t.add_argument("--out", required=True)
+    t.add_argument("--only", nargs="*")
+    t.add_argument("--workload", default="512x512x256")
+    t.add_argument("--steps", type=int, default=20)
+    t.add_argument("--warmup", type=int, default=5)
+    t.add_argument("--cache", default=None)
+    a = ap.parse_args()
+    if a.cmd == "build-variants":
+        for name, lib in build_variants(a.out, a.only).items():
+            print(name, lib)
+    else:
+        name, defines, ms = tune_build(a.workload, a.out, a.only, a.steps, a.warmup, a.cache)
+        print(json.dumps({"workload": a.workload, "best": name, "defines": defines, "ms": ms,
+                          "cache": cache_path(a.cache)}))
+
+
+if __name__ == "__main__":
+    main()

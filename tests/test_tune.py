@@ -43,3 +43,35 @@ def test_candidates():
     assert all(c["fused"] != 1 for c in tune.step_candidates(96, 64))
     modes = {c["mode"] for c in tune.ENSEMBLE_CANDIDATES}
     assert modes == {"sequential", "concurrent", "persistent", "persistent_split"}
+
+
+def test_step_candidates_include_solve_schedules():
+    c = tune.step_candidates(512, 512)
+    assert {"fused": 0, "tdma_reg": 0, "tdma_segments": 0} in c
+    assert {"fused": 0, "tdma_reg": 1, "tdma_segments": 16} in c
+
+
+def test_build_sweep_caches_the_fastest_schedule(tmp_path, monkeypatch):
+    """tune_build times every built variant (here a fake timer keyed by library path),
+    caches every timing and the fastest schedule, and tuned_defines returns its -D list."""
+    out = str(tmp_path / "variants")
+    names = ["default", "cols_4w4l", "rows_pad16"]
+    import os
+    os.makedirs(out)
+    for n in names[1:]:
+        open(tune.variant_path(out, n), "w").close()
+    fake = {None: 5.3, tune.variant_path(out, "cols_4w4l"): 5.9, tune.variant_path(out, "rows_pad16"): 5.1}
+    monkeypatch.setattr(tune, "bench_ms", lambda lib, *a, **k: fake[lib])
+    cache = str(tmp_path / "t.json")
+    name, defines, ms = tune.tune_build("512x512x256", out, names, path=cache, device="B200")
+    assert name == "rows_pad16" and defines == ["OBL_SIDX_SHIFT=4"] and ms == 5.1
+    ent = tune.load_cache(cache)["devices"]["B200"]["build"]["512x512x256"]
+    assert len(ent["timings"]) == 3
+    assert tune.tuned_defines("512x512x256", path=cache) == ["OBL_SIDX_SHIFT=4"]
+    assert tune.tuned_defines("64x64x64", path=cache) == []
+
+
+def test_build_candidates_are_definitions():
+    for name, defs in tune.BUILD_CANDIDATES.items():
+        assert all("=" in d and d.startswith("OBL_") for d in defs), name
+    assert tune.BUILD_CANDIDATES["default"] == []
