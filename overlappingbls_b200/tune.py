@@ -164,8 +164,16 @@ def tune_build(workload, out_dir, names=None, steps=20, warmup=5, path=None, dev
     return best["name"], best["defines"], ms
 
 
+# The schedule sweep's record on this project's B200s, shipped with the package: what
+# ``build --tuned`` uses when the user's cache has no entry for the workload.
+PACKAGED_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_b200.json")
+
+
 def tuned_defines(workload="512x512x256", path=None, device=None):
-    """The -D definitions of the cached fastest schedule for workload ([] if none)."""
+    """The -D definitions of the cached fastest schedule for workload ([] if none); the
+    user's cache first, then the packaged record."""
+    if path is None and not any(workload in d.get("build", {}) for d in load_cache().get("devices", {}).values()):
+        path = PACKAGED_CACHE
     cache = load_cache(path)
     devs = cache.get("devices", {})
     if device is None:
