@@ -156,9 +156,13 @@ def tune_build(workload, out_dir, names=None, steps=20, warmup=5, path=None, dev
             timings.append(({"name": name, "defines": BUILD_CANDIDATES[name]}, None))
             continue
         timings.append(({"name": name, "defines": BUILD_CANDIDATES[name]}, bench_ms(lib, workload, steps, warmup)))
-    best, ms = pick(timings)
     cache = load_cache(path)
     ent = _entry(cache, device, "build")
+    # sweeps may run in parts: timings of candidates not timed now are kept
+    now = {p["name"] for p, _ in timings}
+    old = [(p, t) for p, t in ent.get(workload, {}).get("timings", []) if p["name"] not in now]
+    timings = old + timings
+    best, ms = pick(timings)
     ent[workload] = {"params": best, "ms": ms, "timings": [[p, t] for p, t in timings]}
     save_cache(cache, path)
     return best["name"], best["defines"], ms

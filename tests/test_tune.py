@@ -75,3 +75,19 @@ def test_build_candidates_are_definitions():
     for name, defs in tune.BUILD_CANDIDATES.items():
         assert all("=" in d and d.startswith("OBL_") for d in defs), name
     assert tune.BUILD_CANDIDATES["default"] == []
+
+
+def test_build_sweep_in_parts_merges(tmp_path, monkeypatch):
+    out = str(tmp_path / "v")
+    import os
+    os.makedirs(out)
+    for n in ("cols_4w4l", "rows_pad16"):
+        open(tune.variant_path(out, n), "w").close()
+    fake = {None: 5.3, tune.variant_path(out, "cols_4w4l"): 5.0, tune.variant_path(out, "rows_pad16"): 5.6}
+    monkeypatch.setattr(tune, "bench_ms", lambda lib, *a, **k: fake[lib])
+    cache = str(tmp_path / "t.json")
+    tune.tune_build("w", out, ["default", "cols_4w4l"], path=cache, device="d")
+    name, _, ms = tune.tune_build("w", out, ["default", "rows_pad16"], path=cache, device="d")
+    ent = tune.load_cache(cache)["devices"]["d"]["build"]["w"]
+    assert sorted(p["name"] for p, _ in ent["timings"]) == ["cols_4w4l", "default", "rows_pad16"]
+    assert name == "cols_4w4l" and ms == 5.0
