@@ -72,7 +72,7 @@ template <typename T> int ens_wb();   // lines per CTA of the line-minor column 
 // step in one launch) and the register-class split <0,1,2> (rows), <1,4,4> (columns, solve,
 // y-inverse), <4,6,2> (x-inverse + project).
 #ifndef OBL_ENS_MINB
-#define OBL_ENS_MINB 2   // CTAs per SM the one-launch persistent kernel's registers are bounded for
+#define OBL_ENS_MINB 4   // CTAs per SM the one-launch persistent kernel's registers are bounded for
 #endif
 template <typename T, int PB, int PE, int MINB> struct EnsKernel {
     static cudaError_t attr(size_t smem);
