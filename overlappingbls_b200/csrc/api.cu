@@ -65,6 +65,7 @@ struct obl_ctx {
     DevBuf cscr;               // c' scratch
     DevBuf isl_c, isl_d;
     DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
+    DevBuf hz00;               // G form: (0,0) mode of H_z per level
     DevBuf fscr;               // cluster scratch slots of the fused forward kernel
     // rollout problem of the adjoint: small (ldx,nyt,0:nz) and padded work fields, the
     // per-step state checkpoints and the objective's partial sums
@@ -85,6 +86,7 @@ struct obl_ctx {
     long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
+    long long param_gform = 1;          // pressure RHS: one y-transform of G (1) or of H_x and H_z (0)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t ev[9] = {};
@@ -417,7 +419,35 @@ template <typename T> struct Ops {
             CK(cudaMemsetAsync(Hz + S * (L + 1), 0, sizeof(C2<T>) * S, s()));
         }
         // y c2c (in place), y-Nyquist zeroed
-        if (!rhs_ready) {
+        const bool gf = rhs_ready ? fwd_gform : gform(dpdz_out != nullptr);
+        C2<T> *hz00 = nullptr;
+        if (gf) {
+            // H_y as it is; G = i*kx*H_x + (H_z(z+1) - H_z(z) [+ H_z(0)])/dz formed from the
+            // x-spectra and transformed over H_x; the (0,0) mode of H_z per level; H_z(0)
+            if (!rhs_ready) {
+                auto ca = colargs(Hy + S, lhx, S, Hy + S, lhx, S, lhx, L, 1.0, OP_FWD, ny);
+                ca.zero_nyq = 1;
+                if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
+            }
+            if ((rc = ensure(ctx, ctx->hz00, sizeof(C2<T>) * (size_t)(L + 2)))) return rc;
+            hz00 = (C2<T> *)ctx->hz00.p;
+            {
+                LaunchScope ls(ctx->rec, "press_gform_cols", s());
+                if ((rc = chk(launch_gform_cols<T>(ny, Hx, Hz, ctx->d_kx, S, lhx, L, ctx->dz, twt<T>(ctx, ny, ROLE_FWD),
+                                                   s()),
+                              "press_gform_cols")))
+                    return rc;
+            }
+            {
+                cudaError_t e = cudaSuccess;
+                LaunchScope ls(ctx->rec, "press_hz00", s());
+                launch_hz00<T>(Hz, hz00, S, lhx, ny, L + 2, s(), e);
+                if ((rc = chk(e, "press_hz00"))) return rc;
+            }
+            auto ca = colargs(Hz, lhx, S, Hz, lhx, S, lhx, 1, 1.0, OP_FWD, ny);
+            ca.zero_nyq = 1;
+            if ((rc = cols(OP_FWD, false, ny, ca, "press_bnd_cols"))) return rc;
+        } else if (!rhs_ready) {
             // H_x, H_y levels 1..L in one launch, H_z levels 0..L+1 in another
             MultiPtr<T> m{};
             m.src[0] = m.dst[0] = Hx + S;
@@ -442,7 +472,9 @@ template <typename T> struct Ops {
         ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz;
         ta.dph = dpdz_out ? (C2<T> *)ctx->spec[4].p : nullptr;
         ta.neumann_top = ctx->opt.top_bc == OBL_TOP_NEUMANN;
-        const int P = (ta.neumann_top && ta.dph) ? seg_parts(S, L) : 1;
+        ta.gform = gf ? 1 : 0;
+        ta.hz00 = hz00;
+        const int P = solve_parts(ta.dph != nullptr);
         if (P > 1) {
             // the columns split into segments solved at once (partitioned Thomas, as across
             // z-ranks), then the reduced interface system and the back substitution
@@ -719,7 +751,7 @@ template <typename T> struct Ops {
                               1.0 / ny, OP_PAD, ny);
             if ((rc = cols(OP_PAD, true, ny, ca, "pad_cols"))) return rc;
             if ((rc = ddy((T *)io->d[2 * c + 1], f[c], nlev))) return rc;
-            if (H) {
+            if (H && !(fwd_gform && c != 1)) {   // G form: H_x and H_z are transformed as G in press()
                 auto cb = colargs(H + S, ctx->lhx, S, H + S, ctx->lhx, S, ctx->lhx, ctx->L, 1.0, OP_FWD, ny);
                 cb.zero_nyq = 1;
                 if ((rc = cols(OP_FWD, false, ny, cb, "press_fwd_cols"))) return rc;
@@ -736,6 +768,7 @@ template <typename T> struct Ops {
         // param "fused": 0 multi-output line kernels (default), 1 cluster-fused forward pass,
         // 2 the plain composition of the per-routine entry points
         if (ctx->param_fused == 0 || (ctx->param_fused == 1 && ctx->nxt == ctx->nyt)) {
+            fwd_gform = ctx->param_fused == 0 && gform(true);
             if ((rc = ctx->param_fused == 0 ? fwd_lines(io) : fwd_fused(io))) return rc;
             return press(f[0], f[1], f[2], (const T *)io->divtz_bot, (const T *)io->divtz_top, (T *)io->p,
                          (T *)io->dp[0], (T *)io->dp[1], (T *)io->dp[2], true, io);
@@ -982,6 +1015,17 @@ template <typename T> struct Ops {
         const long long P = std::min<long long>(std::min<long long>(want, kSlabMaxRanks), L / 8);
         return P > 1 ? (int)P : 1;
     }
+    // the solve's column segments for this context (with the spectral dpdz or without)
+    int solve_parts(bool dpdz) const
+    {
+        return (ctx->opt.top_bc == OBL_TOP_NEUMANN && dpdz) ? seg_parts(ctx->sp(), ctx->L) : 1;
+    }
+    // the RHS in G form: the one-sweep and register-segmented solves take it; the
+    // column-segmented solve keeps the three transformed spectra
+    bool gform(bool dpdz) const { return ctx->param_gform && solve_parts(dpdz) == 1; }
+    // set by the step before its line-kernel forward pass: fwd_field leaves H_x and H_z to
+    // press(); the z-slab path, which transforms all three, keeps it false
+    bool fwd_gform = false;
     // the rank's forward pass (ddx, ddy, zero_padding of u,v,w,theta and the RHS spectra),
     // its boundary planes, and a copy of its H_z(1) plane for the rank below
     int slab_begin(const obl_step_io *io, int rank, int P, C2<T> *plane_out)
@@ -1124,6 +1168,8 @@ template <typename T> struct Ops {
         I.Hz = H[2];
         I.S = S;
         TdmaArgs<T> &ta = I.tdma;
+        ta.gform = 0;          // the persistent kernel transforms all three spectra
+        ta.hz00 = nullptr;
         ta.Hx = H[0]; ta.Hy = H[1]; ta.Hz = H[2]; ta.phat = ph; ta.cscr = (T *)ctx->cscr.p;
         ta.kx = ctx->d_kx; ta.ky = ctx->d_ky2; ta.skip = ctx->n_isl ? ctx->d_skip : nullptr;
         ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz; ta.dph = dph;
@@ -1475,6 +1521,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "tdma_segments")) return &ctx->param_tdma_segments;
     if (!std::strcmp(name, "fail_alloc")) return &ctx->param_fail_alloc;
     if (!std::strcmp(name, "tdma_reg")) return &ctx->param_tdma_reg;
+    if (!std::strcmp(name, "gform")) return &ctx->param_gform;
     return nullptr;
 }
 
@@ -2075,6 +2122,7 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
         CK(cudaEventRecord(ctx->ev[c], ci));
     }
     Ops<T> o{ctx};
+    o.fwd_gform = o.gform(true);
     if ((rc = o.fwd_prepare())) return rc;
     for (int c = 0; c < 4; ++c) {
         CK(cudaStreamWaitEvent(s, ctx->ev[c], 0));

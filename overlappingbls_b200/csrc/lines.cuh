@@ -576,16 +576,20 @@ struct NoColEpi {
     __device__ __forceinline__ void prefetch(int, int, int) const {}
 };
 
+// Load hook of the column kernel's input: src(z, i, line) returns element i of global line
+// `line` of plane z in place of the plain load from a.src.  The default is the plain load.
+struct NoColSrc {};
+
 // One CTA unit of the line-minor column kernel: line group bx of plane z.  The plan
 // tables twF/twB are already in shared memory; buf is the exchange scratch (NM*WB).
 // Called by k_cols2 (one unit per CTA) and by the persistent ensemble kernel.
 // tile (SMEM_IN): the unit's input already in shared memory, row i of line l at
 // tile[i*WB + l] (the persistent pipelined kernel below); otherwise read from global.
 template <typename T, int N, int OP, bool REAL, int NW = 8, int WB_ = LmGeo<T>::WB, class EPI = NoColEpi,
-          bool SMEM_IN = false>
+          bool SMEM_IN = false, class SRC = NoColSrc>
 __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, const C2<T> *twF,
                                            const C2<T> *twB, C2<T> *buf, const EPI &epi = EPI(),
-                                           const C2<T> *tile = nullptr)
+                                           const C2<T> *tile = nullptr, const SRC &src = SRC())
 {
     using C = C2<T>;
     using E = typename std::conditional<REAL, T, C>::type;
@@ -604,7 +608,8 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
     const E *srcz = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane;
     E *dstz = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane;
     auto gld = [&](int i) -> C {
-        if constexpr (SMEM_IN) return tile[i * WB + line];
+        if constexpr (!std::is_same<SRC, NoColSrc>::value) return src(z, i, glc);
+        else if constexpr (SMEM_IN) return tile[i * WB + line];
         else if constexpr (REAL) return __ldcg(reinterpret_cast<const C *>(srcz + (long long)i * a.src_row + 2 * glc));
         else return __ldcg(srcz + (long long)i * a.src_row + glc);
     };

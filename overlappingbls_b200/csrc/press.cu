@@ -19,10 +19,10 @@ namespace obl {
 static constexpr double kTadv1 = 1.5;                 // 001_param.f90:152
 static constexpr double kBogus = -1234567890.0;       // 001_param.f90:40
 
-template <typename TS, typename TC, bool ISLAND>
+template <typename TS, typename TC, bool ISLAND, bool G = false>
 __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
 {
-    tdma_column<TS, TC, ISLAND>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+    tdma_column<TS, TC, ISLAND, G>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Mixed precision in one launch: the first nbi blocks solve the FP64 island columns (their
@@ -33,13 +33,13 @@ __global__ void __launch_bounds__(128) k_tdma(TdmaArgs<TS> a, IslandArgs isl)
 #ifndef OBL_TDMA_MINB
 #define OBL_TDMA_MINB 8
 #endif
-template <typename T>
+template <typename T, bool G = false>
 __global__ void __launch_bounds__(128, OBL_TDMA_MINB) k_tdma_mixed(TdmaArgs<T> a, IslandArgs isl, int nbi)
 {
     if ((int)blockIdx.x < nbi)
-        tdma_column<T, double, true>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+        tdma_column<T, double, true, G>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
     else
-        tdma_column<T, T, false>(a, isl, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
+        tdma_column<T, T, false, G>(a, isl, (long long)(blockIdx.x - nbi) * blockDim.x + threadIdx.x);
 }
 
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e)
@@ -47,7 +47,9 @@ template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cud
     if (e != cudaSuccess) return;
     IslandArgs none{nullptr, 0, nullptr, nullptr};
     const int bs = 128;
-    k_tdma<T, T, false><<<(unsigned)((a.S + bs - 1) / bs), bs, 0, s>>>(a, none);
+    const unsigned nb = (unsigned)((a.S + bs - 1) / bs);
+    if (a.gform) k_tdma<T, T, false, true><<<nb, bs, 0, s>>>(a, none);
+    else k_tdma<T, T, false><<<nb, bs, 0, s>>>(a, none);
     e = cudaGetLastError();
 }
 
@@ -57,7 +59,8 @@ void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_
     if (e != cudaSuccess) return;
     const int bs = 128;
     const int nbi = (int)((isl.n + bs - 1) / bs), nbb = (int)((a.S + bs - 1) / bs);
-    k_tdma_mixed<T><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi);
+    if (a.gform) k_tdma_mixed<T, true><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi);
+    else k_tdma_mixed<T><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi);
     e = cudaGetLastError();
 }
 
@@ -80,14 +83,14 @@ constexpr int kRegLev = 16;      // rows a segment keeps in registers (so L <= 2
 
 // NSEG segments (warps) per column; 16 / NSEG CTAs per SM, so fewer levels run with
 // smaller CTAs that overlap one another's load, solve and store phases
-template <typename T, int NSEG>
+template <typename T, int NSEG, bool G>
 __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaArgs<T> a, IslandArgs isl, int nbi,
                                                                           int Ls, int K)
 {
     constexpr int kRegSeg = NSEG;
     using C = C2<T>;
     if ((int)blockIdx.x < nbi) {
-        tdma_column<T, double, true>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+        tdma_column<T, double, true, G>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
         return;
     }
     // boundary coefficients of every segment (x_s = Ys + Vs x_{s-1} + Ws x_{e+1}, same for
@@ -136,25 +139,38 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
         // of the segment's loads are in flight together.
         const long long qc = q;
         hz0 = a.Hz[qc];   // RHS_col(0) = H_z(0) (:209), used by segment 0
-        C hz[kRegLev + 1], hx[kRegLev], hy[kRegLev];
-#pragma unroll
-        for (int i = 0; i <= kRegLev; ++i) hz[i] = __ldcs(a.Hz + qc + S * min(s + i, L + 1));
+        C hx[kRegLev], hy[kRegLev];
 #pragma unroll
         for (int i = 0; i < kRegLev; ++i) {
             const long long zz = min(s + i, L);
             hx[i] = __ldcs(a.Hx + qc + S * zz);
             hy[i] = __ldcs(a.Hy + qc + S * zz);
         }
+        if constexpr (G) {
+            // G + i*ky*H_y; the (0,0) mode takes H_z's own (0,0) value (hz00)
 #pragma unroll
-        for (int i = 0; i < kRegLev; ++i) {
-            const int iz = s + i;
-            const C sxy = mk<T>(kx * hx[i].x + ky * hy[i].x, kx * hx[i].y + ky * hy[i].y);
-            C dh = csub(hz[i + 1], hz[i]);
-            if (iz == 1) dh = cadd(dh, hz0);
-            C r = mk<T>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
-            if (m00) r = (iz == 1) ? mk<T>(0, 0) : hz[i];
-            if (iz == L && !top_solved) r = mk<T>(0, 0);
-            y[i] = r;
+            for (int i = 0; i < kRegLev; ++i) {
+                const int iz = s + i;
+                C r = mk<T>(hx[i].x - ky * hy[i].y, hx[i].y + ky * hy[i].x);
+                if (m00) r = (iz == 1) ? mk<T>(0, 0) : a.hz00[min(iz, L + 1)];
+                if (iz == L && !top_solved) r = mk<T>(0, 0);
+                y[i] = r;
+            }
+        } else {
+            C hz[kRegLev + 1];
+#pragma unroll
+            for (int i = 0; i <= kRegLev; ++i) hz[i] = __ldcs(a.Hz + qc + S * min(s + i, L + 1));
+#pragma unroll
+            for (int i = 0; i < kRegLev; ++i) {
+                const int iz = s + i;
+                const C sxy = mk<T>(kx * hx[i].x + ky * hy[i].x, kx * hx[i].y + ky * hy[i].y);
+                C dh = csub(hz[i + 1], hz[i]);
+                if (iz == 1) dh = cadd(dh, hz0);
+                C r = mk<T>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+                if (m00) r = (iz == 1) ? mk<T>(0, 0) : hz[i];
+                if (iz == L && !top_solved) r = mk<T>(0, 0);
+                y[i] = r;
+            }
         }
         // forward sweep with x_{s-1} left unknown: x_i = y'_i + v'_i x_{s-1} - c'_i x_{i+1}
         T cprev = 0, vprev = 1;
@@ -274,7 +290,8 @@ static void launch_tdma_reg_n(const TdmaArgs<T> &a, const IslandArgs &isl, cudaS
     constexpr int bs = 32 * NSEG;
     const int Ls = (a.L + NSEG - 1) / NSEG, K = (a.L + Ls - 1) / Ls;
     const int nbi = (int)((isl.n + bs - 1) / bs), nbb = (int)((a.S + 31) / 32);
-    k_tdma_reg<T, NSEG><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi, Ls, K);
+    if (a.gform) k_tdma_reg<T, NSEG, true><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi, Ls, K);
+    else k_tdma_reg<T, NSEG, false><<<(unsigned)(nbi + nbb), bs, 0, s>>>(a, isl, nbi, Ls, K);
     e = cudaGetLastError();
 }
 

@@ -18,6 +18,12 @@ template <typename T> struct TdmaArgs {
     int lhx, nyt, L;
     double dz;
     int neumann_top;            // OBL_TOP_NEUMANN
+    // G form (gform = 1): Hx holds the y-transform of G = i*kx*H_x + (H_z(z+1) - H_z(z)
+    // [+ H_z(0) at z = 1])/dz, formed before the transform (kx and the z-difference are
+    // constant along y); H_z is transformed only at level 0; hz00 holds the (0,0) mode of
+    // H_z per level (0..L+1).  The RHS is then G + i*ky*H_y.
+    const C2<T> *hz00;
+    int gform;
 };
 
 // FP64 island work list
@@ -35,7 +41,7 @@ struct IslandArgs {
 constexpr int kTdmaAhead = OBL_TDMA_AHEAD;
 
 // One column's solve; t = the thread's index among the bulk columns or in the island list.
-template <typename TS, typename TC, bool ISLAND>
+template <typename TS, typename TC, bool ISLAND, bool G = false>
 __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandArgs &isl, long long t)
 {
     using CS = C2<TS>;
@@ -104,7 +110,7 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
         const int z = 1 + s;
         rx[s] = raw(a.Hx, z <= L ? z : L);
         ry[s] = raw(a.Hy, z <= L ? z : L);
-        rz[s] = raw(a.Hz, z <= L + 1 ? z : L + 1);
+        if constexpr (!G) rz[s] = raw(a.Hz, z <= L + 1 ? z : L + 1);
     }
     CC dprev = hz0;
     TC cprev = 0;                   // coef_cp(0) = 0 on the bottom rank
@@ -113,13 +119,17 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
         for (int s = 0; s < PF; ++s) {
             const int iz = base + s;
             if (iz > L) break;
-            const CC hx = cv(rx[s]), hy = cv(ry[s]), hzc = cv(rz[s]);
-            const CC hzn = cv(rz[(s + 1) % PF]);   // level iz+1 (slot 0 was refilled at s = 0)
+            const CC hx = cv(rx[s]), hy = cv(ry[s]);
+            CC hzc = mk<TC>(0, 0), hzn = mk<TC>(0, 0);
+            if constexpr (!G) {
+                hzc = cv(rz[s]);
+                hzn = cv(rz[(s + 1) % PF]);   // level iz+1 (slot 0 was refilled at s = 0)
+            }
             {
                 const int zn = iz + PF;
                 rx[s] = raw(a.Hx, zn <= L ? zn : L);
                 ry[s] = raw(a.Hy, zn <= L ? zn : L);
-                rz[s] = raw(a.Hz, zn <= L + 1 ? zn : L + 1);
+                if constexpr (!G) rz[s] = raw(a.Hz, zn <= L + 1 ? zn : L + 1);
             }
             TC am, bm, cm;
             CC r;
@@ -128,15 +138,24 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
                 am = (iz == 1) ? (TC)0 : idz2;
                 bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (TC)2 * idz2);
                 cm = top ? (TC)0 : idz2;
-                const CC sxy = mk<TC>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
-                CC dh = csub(hzn, hzc);
-                if (iz == 1) dh = cadd(dh, hz0);
-                r = mk<TC>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+                if constexpr (G) {
+                    r = mk<TC>(hx.x - ky * hy.y, hx.y + ky * hy.x);   // G + i*ky*H_y
+                } else {
+                    const CC sxy = mk<TC>(kx * hx.x + ky * hy.x, kx * hx.y + ky * hy.y);
+                    CC dh = csub(hzn, hzc);
+                    if (iz == 1) dh = cadd(dh, hz0);
+                    r = mk<TC>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
+                }
             } else {
                 am = (iz == 1) ? (TC)0 : -idz;
                 bm = idz;
                 cm = 0;
-                r = (iz == 1) ? mk<TC>(0, 0) : hzc;
+                if constexpr (G) {
+                    const CS h = a.hz00[iz];
+                    r = (iz == 1) ? mk<TC>(0, 0) : mk<TC>((TC)h.x, (TC)h.y);
+                } else {
+                    r = (iz == 1) ? mk<TC>(0, 0) : hzc;
+                }
             }
             const TC bp = bm - am * cprev;
             const TC ibp = (TC)1 / bp;
@@ -187,7 +206,15 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
     if (dph) dph[S] = mk<TS>((TS)((pn.x - p0.x) / dz), (TS)((pn.y - p0.y) / dz));
 }
 
+// (a.gform selects the G-form instantiations of the solves)
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e);
+// the G-form pieces: the y-transform of G into Hx (levels 1..L, in place) and the (0,0)
+// mode of H_z per level 0..L+1 (the sum over y of the kx = 0 column of the x-spectra)
+template <typename T>
+cudaError_t launch_gform_cols(int ny, C2<T> *Hx, const C2<T> *Hz, const double *kx, long long S, int lhx, int L,
+                              double dz, const C2<T> *twF, cudaStream_t s);
+template <typename T> void launch_hz00(const C2<T> *Hz, C2<T> *hz00, long long S, int lhx, int ny, int nlev,
+                                       cudaStream_t s, cudaError_t &e);
 // FP32 bulk columns by the register-segmented partitioned solve (no scratch traffic),
 // FP64 island columns (isl.n may be 0) by the sequential FP64 sweep in the same launch;
 // levels L <= 256
