@@ -65,7 +65,6 @@ struct obl_ctx {
     DevBuf cscr;               // c' scratch
     DevBuf isl_c, isl_d;
     DevBuf tmp;                // pad/unpad intermediate, ifftn temporary
-    DevBuf hz00;               // G form: (0,0) mode of H_z per level
     DevBuf fscr;               // cluster scratch slots of the fused forward kernel
     // rollout problem of the adjoint: small (ldx,nyt,0:nz) and padded work fields, the
     // per-step state checkpoints and the objective's partial sums
@@ -420,17 +419,15 @@ template <typename T> struct Ops {
         }
         // y c2c (in place), y-Nyquist zeroed
         const bool gf = rhs_ready ? fwd_gform : gform(dpdz_out != nullptr);
-        C2<T> *hz00 = nullptr;
         if (gf) {
             // H_y as it is; G = i*kx*H_x + (H_z(z+1) - H_z(z) [+ H_z(0)])/dz formed from the
-            // x-spectra and transformed over H_x; the (0,0) mode of H_z per level; H_z(0)
+            // x-spectra and transformed over H_x; H_z at level 0, and at levels 1..L only in
+            // the line group of kx = 0 (the (0,0) mode's RHS, the same transform as before)
             if (!rhs_ready) {
                 auto ca = colargs(Hy + S, lhx, S, Hy + S, lhx, S, lhx, L, 1.0, OP_FWD, ny);
                 ca.zero_nyq = 1;
                 if ((rc = cols(OP_FWD, false, ny, ca, "press_fwd_cols"))) return rc;
             }
-            if ((rc = ensure(ctx, ctx->hz00, sizeof(C2<T>) * (size_t)(L + 2)))) return rc;
-            hz00 = (C2<T> *)ctx->hz00.p;
             {
                 LaunchScope ls(ctx->rec, "press_gform_cols", s());
                 if ((rc = chk(launch_gform_cols<T>(ny, Hx, Hz, ctx->d_kx, S, lhx, L, ctx->dz, twt<T>(ctx, ny, ROLE_FWD),
@@ -438,15 +435,12 @@ template <typename T> struct Ops {
                               "press_gform_cols")))
                     return rc;
             }
-            {
-                cudaError_t e = cudaSuccess;
-                LaunchScope ls(ctx->rec, "press_hz00", s());
-                launch_hz00<T>(Hz, hz00, S, lhx, ny, L + 2, s(), e);
-                if ((rc = chk(e, "press_hz00"))) return rc;
-            }
             auto ca = colargs(Hz, lhx, S, Hz, lhx, S, lhx, 1, 1.0, OP_FWD, ny);
             ca.zero_nyq = 1;
             if ((rc = cols(OP_FWD, false, ny, ca, "press_bnd_cols"))) return rc;
+            auto c0 = colargs(Hz + S, lhx, S, Hz + S, lhx, S, 1, L, 1.0, OP_FWD, ny);   // column kx = 0
+            c0.zero_nyq = 1;
+            if ((rc = cols(OP_FWD, false, ny, c0, "press_mean_cols"))) return rc;
         } else if (!rhs_ready) {
             // H_x, H_y levels 1..L in one launch, H_z levels 0..L+1 in another
             MultiPtr<T> m{};
@@ -473,7 +467,6 @@ template <typename T> struct Ops {
         ta.dph = dpdz_out ? (C2<T> *)ctx->spec[4].p : nullptr;
         ta.neumann_top = ctx->opt.top_bc == OBL_TOP_NEUMANN;
         ta.gform = gf ? 1 : 0;
-        ta.hz00 = hz00;
         const int P = solve_parts(ta.dph != nullptr);
         if (P > 1) {
             // the columns split into segments solved at once (partitioned Thomas, as across
@@ -1169,7 +1162,6 @@ template <typename T> struct Ops {
         I.S = S;
         TdmaArgs<T> &ta = I.tdma;
         ta.gform = 0;          // the persistent kernel transforms all three spectra
-        ta.hz00 = nullptr;
         ta.Hx = H[0]; ta.Hy = H[1]; ta.Hz = H[2]; ta.phat = ph; ta.cscr = (T *)ctx->cscr.p;
         ta.kx = ctx->d_kx; ta.ky = ctx->d_ky2; ta.skip = ctx->n_isl ? ctx->d_skip : nullptr;
         ta.S = S; ta.lhx = lhx; ta.nyt = ny; ta.L = L; ta.dz = ctx->dz; ta.dph = dph;

@@ -7,7 +7,7 @@ namespace obl {
 
 // k_cols2 for OP_DERIV on real columns, with the DivEpi store hook
 template <typename T, int N, int NW, int WB, bool TWG>
-__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG)) k_cols_divt(ColArgs<T> a, DivEpi<T> e)
+__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG, col_warps_sm<OP_DERIV>())) k_cols_divt(ColArgs<T> a, DivEpi<T> e)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_DERIV>;

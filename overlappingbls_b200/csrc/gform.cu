@@ -7,9 +7,9 @@
 //     G = i*kx*H_x + (H_z(z+1) - H_z(z) [+ H_z(0)])/dz
 // can be formed from the x-spectra before it: one y-transform of G (written over H_x)
 // replaces those of H_x and H_z, and the solve forms G + i*ky*H_y.  H_z is still
-// transformed at level 0 (the Neumann ghost p_hat(0) = p_hat(1) - dz*H_z(0), :313-315),
-// and the (0,0) mode, whose RHS is H_z itself (:219-221), takes the y-sum of the kx = 0
-// column of each level's x-spectrum (hz00).
+// transformed at level 0 (the Neumann ghost p_hat(0) = p_hat(1) - dz*H_z(0), :313-315)
+// and, at levels 1..L, in the line group of kx = 0 only: the (0,0) mode's RHS is H_z
+// itself (:219-221).
 #include "lines_dispatch.cuh"
 #include "press.cuh"
 
@@ -36,7 +36,7 @@ template <typename T, bool FIRST> struct GSrc {
 };
 
 template <typename T, int N, int NW, int WB, bool TWG, bool FIRST>
-__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG)) k_cols_gform(ColArgs<T> a, GSrc<T, FIRST> g)
+__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG, col_warps_sm<OP_FWD>())) k_cols_gform(ColArgs<T> a, GSrc<T, FIRST> g)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP_FWD>;
@@ -115,52 +115,9 @@ cudaError_t launch_gform_cols(int ny, C2<T> *Hx, const C2<T> *Hz, const double *
     return cudaSuccess;
 }
 
-// (0,0) mode of H_z per level: the sum over y of the kx = 0 column of its x-spectrum (the
-// ky = 0 bin of the y-transform), accumulated in FP64; one block per level
-template <typename T> __global__ void __launch_bounds__(256) k_hz00(const C2<T> *Hz, C2<T> *hz00, long long S, int lhx, int ny)
-{
-    __shared__ double red[2][8];
-    const long long lv = blockIdx.x;
-    double sx = 0, sy = 0;
-    for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-        const C2<T> h = Hz[S * lv + (long long)y * lhx];
-        sx += (double)h.x;
-        sy += (double)h.y;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        sx += __shfl_down_sync(0xffffffffu, sx, o);
-        sy += __shfl_down_sync(0xffffffffu, sy, o);
-    }
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        red[0][w] = sx;
-        red[1][w] = sy;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tx = 0, ty = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-            tx += red[0][k];
-            ty += red[1][k];
-        }
-        hz00[lv] = mk<T>((T)tx, (T)ty);
-    }
-}
-
-template <typename T>
-void launch_hz00(const C2<T> *Hz, C2<T> *hz00, long long S, int lhx, int ny, int nlev, cudaStream_t s, cudaError_t &e)
-{
-    if (e != cudaSuccess || nlev < 1) return;
-    k_hz00<T><<<nlev, 256, 0, s>>>(Hz, hz00, S, lhx, ny);
-    e = cudaGetLastError();
-}
-
 template cudaError_t launch_gform_cols<float>(int, C2<float> *, const C2<float> *, const double *, long long, int, int,
                                               double, const C2<float> *, cudaStream_t);
 template cudaError_t launch_gform_cols<double>(int, C2<double> *, const C2<double> *, const double *, long long, int,
                                                int, double, const C2<double> *, cudaStream_t);
-template void launch_hz00<float>(const C2<float> *, C2<float> *, long long, int, int, int, cudaStream_t, cudaError_t &);
-template void launch_hz00<double>(const C2<double> *, C2<double> *, long long, int, int, int, cudaStream_t,
-                                  cudaError_t &);
 
 } // namespace obl

@@ -554,10 +554,14 @@ template <typename T, int N, int OP> constexpr int col_lines()
 #ifndef OBL_COL_WARPS_SM
 #define OBL_COL_WARPS_SM 32   // resident warps per SM the register bound is set for
 #endif
-constexpr int col_min_blocks(int nw, bool twg)
+#ifndef OBL_COLS_WARPS_SM
+#define OBL_COLS_WARPS_SM OBL_COL_WARPS_SM   // the same for ddy and the y-transform alone
+#endif
+constexpr int col_min_blocks(int nw, bool twg, int warps_sm = OBL_COL_WARPS_SM)
 {
-    return twg ? (nw >= OBL_COL_WARPS_SM ? 1 : OBL_COL_WARPS_SM / nw) : 1;
+    return twg ? (nw >= warps_sm ? 1 : warps_sm / nw) : 1;
 }
+template <int OP> constexpr int col_warps_sm() { return (OP == OP_DERIV || OP == OP_FWD) ? OBL_COLS_WARPS_SM : OBL_COL_WARPS_SM; }
 
 template <typename T, int N, int OP, int NW = 8, int WB = LmGeo<T>::WB> struct ColDerived {
     using D = LineDerived<N, OP>;
@@ -744,7 +748,7 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
 }
 
 template <typename T, int N, int OP, bool REAL, int NW, int WB, bool TWG = false>
-__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG)) k_cols2(ColArgs<T> a)
+__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG, col_warps_sm<OP>())) k_cols2(ColArgs<T> a)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP>;

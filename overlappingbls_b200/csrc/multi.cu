@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(256) k_rows_multi(RowArgs<T> a0, MultiPtr<T> m
 }
 
 template <typename T, int N, int OP, bool REAL, int NW, int WB, bool TWG>
-__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG)) k_cols2_multi(ColArgs<T> a0, MultiPtr<T> m)
+__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, TWG, col_warps_sm<OP>())) k_cols2_multi(ColArgs<T> a0, MultiPtr<T> m)
 {
     using C = C2<T>;
     using D = LineDerived<N, OP>;

@@ -147,12 +147,12 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
             hy[i] = __ldcs(a.Hy + qc + S * zz);
         }
         if constexpr (G) {
-            // G + i*ky*H_y; the (0,0) mode takes H_z's own (0,0) value (hz00)
+            // G + i*ky*H_y; the (0,0) mode takes H_z's own (0,0) value (q = 0)
 #pragma unroll
             for (int i = 0; i < kRegLev; ++i) {
                 const int iz = s + i;
                 C r = mk<T>(hx[i].x - ky * hy[i].y, hx[i].y + ky * hy[i].x);
-                if (m00) r = (iz == 1) ? mk<T>(0, 0) : a.hz00[min(iz, L + 1)];
+                if (m00) r = (iz == 1) ? mk<T>(0, 0) : a.Hz[S * min(iz, L + 1)];
                 if (iz == L && !top_solved) r = mk<T>(0, 0);
                 y[i] = r;
             }

@@ -20,9 +20,8 @@ template <typename T> struct TdmaArgs {
     int neumann_top;            // OBL_TOP_NEUMANN
     // G form (gform = 1): Hx holds the y-transform of G = i*kx*H_x + (H_z(z+1) - H_z(z)
     // [+ H_z(0) at z = 1])/dz, formed before the transform (kx and the z-difference are
-    // constant along y); H_z is transformed only at level 0; hz00 holds the (0,0) mode of
-    // H_z per level (0..L+1).  The RHS is then G + i*ky*H_y.
-    const C2<T> *hz00;
+    // constant along y); H_z is transformed at level 0 and, at levels 1..L, only in the
+    // line group of kx = 0 (the (0,0) mode's RHS).  The RHS is then G + i*ky*H_y.
     int gform;
 };
 
@@ -151,8 +150,7 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
                 bm = idz;
                 cm = 0;
                 if constexpr (G) {
-                    const CS h = a.hz00[iz];
-                    r = (iz == 1) ? mk<TC>(0, 0) : mk<TC>((TC)h.x, (TC)h.y);
+                    r = (iz == 1) ? mk<TC>(0, 0) : cv(raw(a.Hz, iz));   // q = 0: the (0,0) mode
                 } else {
                     r = (iz == 1) ? mk<TC>(0, 0) : hzc;
                 }
@@ -208,13 +206,10 @@ __device__ __forceinline__ void tdma_column(const TdmaArgs<TS> &a, const IslandA
 
 // (a.gform selects the G-form instantiations of the solves)
 template <typename T> void launch_tdma(const TdmaArgs<T> &a, cudaStream_t s, cudaError_t &e);
-// the G-form pieces: the y-transform of G into Hx (levels 1..L, in place) and the (0,0)
-// mode of H_z per level 0..L+1 (the sum over y of the kx = 0 column of the x-spectra)
+// the G form's y-transform of G into Hx (levels 1..L, in place)
 template <typename T>
 cudaError_t launch_gform_cols(int ny, C2<T> *Hx, const C2<T> *Hz, const double *kx, long long S, int lhx, int L,
                               double dz, const C2<T> *twF, cudaStream_t s);
-template <typename T> void launch_hz00(const C2<T> *Hz, C2<T> *hz00, long long S, int lhx, int ny, int nlev,
-                                       cudaStream_t s, cudaError_t &e);
 // FP32 bulk columns by the register-segmented partitioned solve (no scratch traffic),
 // FP64 island columns (isl.n may be 0) by the sequential FP64 sweep in the same launch;
 // levels L <= 256
