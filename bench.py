@@ -207,8 +207,7 @@ def algorithmic_bytes(name, info, s):
         "press_fwd_cols": 2 * lhx * ny * L * c,
         "tdma": 5 * lhx * ny * L * c,
         "tdma_mixed": 5 * lhx * ny * L * c,
-        # the step's solve reads G and H_y (the RHS in G form) and writes p_hat and dpdz's spectrum
-        "tdma_reg": 4 * lhx * ny * L * c,
+        "tdma_reg": 5 * lhx * ny * L * c,
         # levels 1..L of H_x and 0..L+1 of H_z in, the y-transform of G over H_x out (2 launches)
         "press_gform_cols": ((L + (L + 2) + L) * lhx * ny * c) / 2,
         # one launch per field: field in, ddx and the x-padded rows out, and on u, v, w the

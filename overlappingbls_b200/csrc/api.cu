@@ -85,7 +85,7 @@ struct obl_ctx {
     long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
-    long long param_gform = 1;          // pressure RHS: one y-transform of G (1) or of H_x and H_z (0)
+    long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t ev[9] = {};
@@ -1014,8 +1014,14 @@ template <typename T> struct Ops {
         return (ctx->opt.top_bc == OBL_TOP_NEUMANN && dpdz) ? seg_parts(ctx->sp(), ctx->L) : 1;
     }
     // the RHS in G form: the one-sweep and register-segmented solves take it; the
-    // column-segmented solve keeps the three transformed spectra
-    bool gform(bool dpdz) const { return ctx->param_gform && solve_parts(dpdz) == 1; }
+    // column-segmented solve keeps the three transformed spectra.  By default only with
+    // FP64 storage: the RHS is a divergence whose terms nearly cancel, and G's partial sum
+    // rounded to FP32 before the transform costs the FP64 island columns their exact RHS
+    // assembly (at 512^2 x 256 the mixed form's p error rose from 1.4e-7 to 8.5e-6).
+    bool gform(bool dpdz) const
+    {
+        return (ctx->param_gform == 2 || (ctx->param_gform == 1 && ctx->f64)) && solve_parts(dpdz) == 1;
+    }
     // set by the step before its line-kernel forward pass: fwd_field leaves H_x and H_z to
     // press(); the z-slab path, which transforms all three, keeps it false
     bool fwd_gform = false;

@@ -255,8 +255,9 @@ def test_step_factor5_lengths(orc, prec, nx, ny, nzt):
 @pytest.mark.parametrize("top", ["neumann", "single"])
 def test_rhs_in_g_form(orc, prec, top):
     """The pressure RHS formed as G = i*kx*H_x + dz-difference of H_z before one
-    y-transform (G form) against the three separately transformed spectra and against the
-    oracle, with divtz boundary planes (a grid whose solve runs as one sweep per column)."""
+    y-transform (G form, forced with gform = 2; by default it runs with FP64 storage only)
+    against the three separately transformed spectra and against the oracle, with divtz
+    boundary planes (a grid whose solve runs as one sweep per column)."""
     nx, ny, nzt = 512, 256, 33
     ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
     f = identical_inputs(fields.make_fields(nx, ny, nzt), prec)
@@ -264,7 +265,7 @@ def test_rhs_in_g_form(orc, prec, top):
     pl = identical_inputs({k: np.asfortranarray(0.1 * rng.standard_normal((ctx.ldx, ny))) for k in ("b", "t")}, prec)
     L = ctx.nz - 1
     outs = {}
-    for gf in (1, 0):
+    for gf in (2, 0):
         ctx.set_param("gform", gf)
         u, v, w = (f[k].copy(order="F") for k in "uvw")
         d, big, p, dp = _alloc_step(ctx)
@@ -275,12 +276,14 @@ def test_rhs_in_g_form(orc, prec, top):
     rp, rdx, rdy = g.press_stag_array(f["u"], f["v"], f["w"], pl["b"], pl["t"], npz=npz)
     rdz = g.dpdz(rp)
     ru, rv, rw = g.project(f["u"], f["v"], f["w"], rdx, rdy, rdz)
-    for gf in (1, 0):
+    for gf in (2, 0):
         p, dp, u, v, w = outs[gf]
         assert rel_l2(p[:nx, :, : L + 1], rp[:nx, :, : L + 1]) < TOL[prec], gf
         for a, r in zip(dp, (rdx, rdy, rdz)):
             assert rel_l2(a[:nx, :, :L], r[:nx, :, :L]) < TOL[prec], gf
         for a, r in ((u, ru), (v, rv), (w, rw)):
             assert rel_l2(a, r) < TOL[prec], gf
-    tol = 1e-12 if prec == "f64" else 2e-6
-    assert rel_l2(outs[1][0][:nx, :, : L + 1], outs[0][0][:nx, :, : L + 1]) < tol
+    # mixed: G's partial sum is rounded to FP32 before the transform (the RHS terms nearly
+    # cancel), so the two forms agree only to the oracle's tolerance
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel_l2(outs[2][0][:nx, :, : L + 1], outs[0][0][:nx, :, : L + 1]) < tol
