@@ -86,8 +86,9 @@ struct obl_ctx {
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
+    long long param_out_streams = 1;    // host step: device -> host copy streams (1 or 2)
     // overlapped host step: input and output copy streams, per-field events
-    cudaStream_t cin = nullptr, cout = nullptr;
+    cudaStream_t cin = nullptr, cout = nullptr, cout2 = nullptr;
     cudaEvent_t ev[9] = {};
     std::vector<DevBuf> stage; // host-variant staging (storage type)
     std::vector<DevBuf> stage64;
@@ -1468,6 +1469,7 @@ int obl_ctx_destroy(obl_ctx *ctx)
     for (auto &b : ctx->stage64) cudaFree(b.p);
     if (ctx->cin) cudaStreamDestroy(ctx->cin);
     if (ctx->cout) cudaStreamDestroy(ctx->cout);
+    if (ctx->cout2) cudaStreamDestroy(ctx->cout2);
     for (auto e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;
@@ -1520,6 +1522,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "fail_alloc")) return &ctx->param_fail_alloc;
     if (!std::strcmp(name, "tdma_reg")) return &ctx->param_tdma_reg;
     if (!std::strcmp(name, "gform")) return &ctx->param_gform;
+    if (!std::strcmp(name, "out_streams")) return &ctx->param_out_streams;
     return nullptr;
 }
 
@@ -2058,6 +2061,7 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
         CK(cudaStreamCreateWithFlags(&ctx->cout, cudaStreamNonBlocking));
         for (auto &e : ctx->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
+    if (ctx->param_out_streams > 1 && !ctx->cout2) CK(cudaStreamCreateWithFlags(&ctx->cout2, cudaStreamNonBlocking));
     // device buffers: the staging slots of the staged path (same layout)
     const long long n[22] = {nf, nf, nf, nf, nf, nf, nf, nf, nf, nf, nf, nf, nb, nb, nb, nb, nf, nd, nd, nd, pl, pl};
     const void *h[22] = {io->u, io->v, io->w, io->theta, io->d[0], io->d[1], io->d[2], io->d[3], io->d[4], io->d[5],
@@ -2086,7 +2090,10 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
     for (int i = 0; i < 3; ++i) dio.dp[i] = d[17 + i];
     dio.divtz_bot = d[20];
     dio.divtz_top = d[21];
-    const cudaStream_t s = ctx->stream, ci = ctx->cin, co = ctx->cout;
+    const cudaStream_t s = ctx->stream, ci = ctx->cin;
+    // the outputs alternate between the copy streams (two DMA engines when there are two)
+    const cudaStream_t cos[2] = {ctx->cout, ctx->param_out_streams > 1 ? ctx->cout2 : ctx->cout};
+    int nout = 0;
     // host type -> storage type (or storage -> host) of n elements on stream st
     auto convert = [&](void *dst, const void *src, long long cnt, bool to_storage, cudaStream_t st) -> cudaError_t {
         cudaError_t e = cudaSuccess;
@@ -2103,6 +2110,7 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
     };
     // rows [row0, row0+nrows) of pitch ld, the first width elements of each (x < nxt)
     auto out = [&](int i, long long ld, long long width, long long row0, long long nrows) -> cudaError_t {
+        const cudaStream_t co = cos[(nout++) & 1];
         if (conv) {
             cudaError_t e = convert((HT *)l[i] + row0 * ld, (const T *)d[i] + row0 * ld, ld * nrows, false, co);
             if (e != cudaSuccess) return e;
@@ -2126,7 +2134,7 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
         CK(cudaStreamWaitEvent(s, ctx->ev[c], 0));
         if ((rc = o.fwd_field(&dio, c))) return rc;
         CK(cudaEventRecord(ctx->ev[4 + c], s));
-        CK(cudaStreamWaitEvent(co, ctx->ev[4 + c], 0));
+        for (cudaStream_t co : cos) CK(cudaStreamWaitEvent(co, ctx->ev[4 + c], 0));
         CK(out(4 + 2 * c, ctx->ldx, ctx->nxt, 0, ny * nlev));
         CK(out(5 + 2 * c, ctx->ldx, ctx->nxt, 0, ny * nlev));
         CK(out(12 + c, nb, nb, 0, 1));
@@ -2135,11 +2143,11 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
                       (const T *)dio.divtz_top, (T *)dio.p, (T *)dio.dp[0], (T *)dio.dp[1], (T *)dio.dp[2], true, &dio)))
         return rc;
     CK(cudaEventRecord(ctx->ev[8], s));
-    CK(cudaStreamWaitEvent(co, ctx->ev[8], 0));
+    for (cudaStream_t co : cos) CK(cudaStreamWaitEvent(co, ctx->ev[8], 0));
     CK(out(16, ctx->ldx, ctx->nxt, 0, ny * (L + 1)));
     for (int i = 0; i < 3; ++i) CK(out(17 + i, ctx->ldx, ctx->nxt, 0, ny * L));
     for (int i = 0; i < 3; ++i) CK(out(i, nf, nf, 0, 1));
-    CK(cudaStreamSynchronize(co));
+    for (cudaStream_t co : cos) CK(cudaStreamSynchronize(co));
     CK(cudaStreamSynchronize(s));
     return OBL_OK;
 }
