@@ -86,7 +86,7 @@ struct obl_ctx {
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
-    long long param_out_streams = 1;    // host step: device -> host copy streams (1 or 2)
+    long long param_out_streams = 2;    // host step: device -> host copy streams (1 or 2)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr, cout2 = nullptr;
     cudaEvent_t ev[9] = {};
