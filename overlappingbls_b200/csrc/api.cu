@@ -87,6 +87,7 @@ struct obl_ctx {
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
     long long param_out_streams = 2;    // host step: device -> host copy streams (1 or 2)
+    long long param_fwd_chunk = 0;      // forward pass in chunks of this many levels (0 = whole fields)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr, cout2 = nullptr;
     cudaEvent_t ev[9] = {};
@@ -724,16 +725,20 @@ template <typename T> struct Ops {
     int fwd_field(const obl_step_io *io, int c)
     {
         const int nlev = ctx->nz + 1, nx = ctx->nxt, ny = ctx->nyt, nx2 = ctx->nxt2, ny2 = ctx->nyt2;
-        const long long S = ctx->sp();
+        const long long S = ctx->sp(), pl = ctx->plane(), plb = (long long)nx2 * ny2;
         int rc;
         T *xb = (T *)ctx->tmp.p;
         const T *f[4] = {(const T *)io->u, (const T *)io->v, (const T *)io->w, (const T *)io->theta};
         const double scp = ((1.0 / ((double)nx * ny)) / kTadv1) * (1.0 / ctx->dt_nd);
-        {
-            C2<T> *H = c < 3 ? (C2<T> *)ctx->spec[c].p : nullptr;
+        C2<T> *H = c < 3 ? (C2<T> *)ctx->spec[c].p : nullptr;
+        // chunks of levels (fwd_chunk): the chunk's x-padded planes reuse the start of the
+        // intermediate and the field rows are re-read by ddy while they may still be in L2
+        const int ch = ctx->param_fwd_chunk > 0 ? (int)std::min<long long>(ctx->param_fwd_chunk, nlev) : nlev;
+        for (int z0 = 0; z0 < nlev; z0 += ch) {
+            const int nl = std::min(ch, nlev - z0);
             RowsFwd3Args<T> ra{};
-            ra.src = f[c]; ra.dfdx = (T *)io->d[2 * c]; ra.xpad = xb; ra.H = H;
-            ra.npairs = (long long)ny * nlev / 2; ra.ldx = ctx->ldx; ra.ny = ny; ra.L = ctx->L;
+            ra.src = f[c] + pl * z0; ra.dfdx = (T *)io->d[2 * c] + pl * z0; ra.xpad = xb; ra.H = H ? H + S * z0 : nullptr;
+            ra.npairs = (long long)ny * nl / 2; ra.ldx = ctx->ldx; ra.ny = ny; ra.L = ctx->L; ra.z0 = z0;
             ra.sc_press = scp; ra.kx = ctx->d_kx;
             ra.twF = twt<T>(ctx, nx, ROLE_FWD); ra.twB = twt<T>(ctx, nx, ROLE_BWD);
             ra.twPB = twt<T>(ctx, nx, ROLE_PADBWD);
@@ -741,14 +746,19 @@ template <typename T> struct Ops {
                 LaunchScope ls(ctx->rec, "rows_fwd3", s());
                 if ((rc = chk(RowsFwd3Launch<T>::run(nx, ra, s()), "rows_fwd3"))) return rc;
             }
-            auto ca = colargs(xb, nx2, (long long)nx2 * ny, io->big[c], nx2, (long long)nx2 * ny2, nx2, nlev,
+            auto ca = colargs(xb, nx2, (long long)nx2 * ny, (T *)io->big[c] + plb * z0, nx2, plb, nx2, nl,
                               1.0 / ny, OP_PAD, ny);
             if ((rc = cols(OP_PAD, true, ny, ca, "pad_cols"))) return rc;
-            if ((rc = ddy((T *)io->d[2 * c + 1], f[c], nlev))) return rc;
+            if ((rc = ddy((T *)io->d[2 * c + 1] + pl * z0, f[c] + pl * z0, nl))) return rc;
             if (H && !(fwd_gform && c != 1)) {   // G form: H_x and H_z are transformed as G in press()
-                auto cb = colargs(H + S, ctx->lhx, S, H + S, ctx->lhx, S, ctx->lhx, ctx->L, 1.0, OP_FWD, ny);
-                cb.zero_nyq = 1;
-                if ((rc = cols(OP_FWD, false, ny, cb, "press_fwd_cols"))) return rc;
+                // RHS levels 1..L of this chunk
+                const int a0 = std::max(z0, 1), a1 = std::min(z0 + nl - 1, ctx->L);
+                if (a1 >= a0) {
+                    auto cb = colargs(H + S * a0, ctx->lhx, S, H + S * a0, ctx->lhx, S, ctx->lhx, a1 - a0 + 1, 1.0,
+                                      OP_FWD, ny);
+                    cb.zero_nyq = 1;
+                    if ((rc = cols(OP_FWD, false, ny, cb, "press_fwd_cols"))) return rc;
+                }
             }
         }
         return OBL_OK;
@@ -1147,7 +1157,7 @@ template <typename T> struct Ops {
             T *xb = xpad4 + (size_t)c * nx2 * ny * nlev;
             RowsFwd3Args<T> &ra = I.rows[c];
             ra.src = f[c]; ra.dfdx = (T *)io->d[2 * c]; ra.xpad = xb; ra.H = c < 3 ? H[c] : nullptr;
-            ra.npairs = (long long)ny * nlev / 2; ra.ldx = ldx; ra.ny = ny; ra.L = L;
+            ra.npairs = (long long)ny * nlev / 2; ra.ldx = ldx; ra.ny = ny; ra.L = L; ra.z0 = 0;
             ra.sc_press = scp; ra.kx = ctx->d_kx;
             ra.twF = twt<T>(ctx, nx, ROLE_FWD); ra.twB = twt<T>(ctx, nx, ROLE_BWD);
             ra.twPB = twt<T>(ctx, nx, ROLE_PADBWD);
@@ -1523,6 +1533,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "tdma_reg")) return &ctx->param_tdma_reg;
     if (!std::strcmp(name, "gform")) return &ctx->param_gform;
     if (!std::strcmp(name, "out_streams")) return &ctx->param_out_streams;
+    if (!std::strcmp(name, "fwd_chunk")) return &ctx->param_fwd_chunk;
     return nullptr;
 }
 

@@ -263,6 +263,7 @@ template <typename T> struct RowsFwd3Args {
     C2<T> *H;              // (lhx, ny, nlev) or nullptr (theta)
     long long npairs;      // ny*nlev/2
     int ldx, ny, L;
+    int z0;                // level of the first row pair (src, dfdx, H start there; a chunk of levels)
     double sc_press;
     const double *kx;
     const C2<T> *twF, *twB, *twPB;
@@ -289,7 +290,7 @@ __device__ __forceinline__ void rows_fwd3_unit(const RowsFwd3Args<T> &a, long lo
         const bool act = p < a.npairs;
         const long long r0 = 2 * (act ? p : base);
         // warp-uniform: the LPW pairs of a warp lie on one level (ny/2 is a multiple of LPW)
-        const int zw = (int)((2 * base) / a.ny);
+        const int zw = a.z0 + (int)((2 * base) / a.ny);
         const bool spec = a.H != nullptr && zw >= 1 && zw <= a.L;
         const T *A = a.src + r0 * a.ldx;
         T *dA = a.dfdx + r0 * a.ldx;

@@ -287,3 +287,23 @@ def test_rhs_in_g_form(orc, prec, top):
     # cancel), so the two forms agree only to the oracle's tolerance
     tol = 1e-12 if prec == "f64" else 1e-5
     assert rel_l2(outs[2][0][:nx, :, : L + 1], outs[0][0][:nx, :, : L + 1]) < tol
+
+
+@pytest.mark.parametrize("chunk", [1, 7, 64])
+def test_forward_pass_in_level_chunks(orc, chunk):
+    """The line-kernel forward pass run in chunks of levels (fwd_chunk: 1, 7 and 64 levels
+    of 66 stored ones) gives the same step as the whole-field pass."""
+    nx, ny, nzt = 128, 96, 65
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), "mixed")
+    outs = []
+    for ch in (0, chunk):
+        ctx = obl.Context(nx, ny, nzt, precision="mixed", top_bc="neumann", **fields.DOMAIN)
+        ctx.set_param("fwd_chunk", ch)
+        u, v, w = (f[k].copy(order="F") for k in "uvw")
+        d, big, p, dp = _alloc_step(ctx)
+        ctx.step(u, v, w, f["theta"], d, big, p, dp)
+        outs.append((d, big, p, dp, u, v, w))
+        ctx.close()
+    (d0, b0, p0, dp0, *uvw0), (d1, b1, p1, dp1, *uvw1) = outs
+    for a, b in zip(d1 + b1 + [p1] + dp1 + uvw1, d0 + b0 + [p0] + dp0 + uvw0):
+        assert np.array_equal(a, b)
