@@ -10,6 +10,7 @@
 // On one GPU the pipelined send/recv chain across z-ranks collapses to one sequential
 // sweep per column, which is the same arithmetic in the same order.
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 #include "press.cuh"
@@ -79,6 +80,19 @@ void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_
 // 4-63, 203-225, 280-317); the rows are the same, only the elimination order differs.
 // FP64 island columns keep the sequential FP64 sweep, in the launch's first nbi blocks.
 constexpr int kRegSegMax = 16;   // warps per CTA = segments per column, at most
+
+// 1/x for the FP32 columns' recurrences: the hardware reciprocal (__fdividef, within 2 ulp)
+// instead of the IEEE division sequence, which sat on the sweep's serial dependency chain;
+// the FP32 columns are diagonally dominant and round at 6e-8 anyway (the weakly dominant
+// ones are the FP64 islands)
+#ifndef OBL_TDMA_FAST_RCP
+#define OBL_TDMA_FAST_RCP 1
+#endif
+template <typename T> __device__ __forceinline__ T rcp_sweep(T x)
+{
+    if constexpr (std::is_same<T, float>::value && OBL_TDMA_FAST_RCP) return __fdividef(1.0f, x);
+    else return (T)1 / x;
+}
 constexpr int kRegLev = 16;      // rows a segment keeps in registers (so L <= 256)
 
 // NSEG segments (warps) per column; 16 / NSEG CTAs per SM, so fewer levels run with
@@ -192,7 +206,7 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
                     bm = idz;
                     cm = 0;
                 }
-                const T ibp = (T)1 / (bm - am * cprev);
+                const T ibp = rcp_sweep<T>(bm - am * cprev);
                 cp[i] = cm * ibp;
                 vp[i] = -am * vprev * ibp;
                 y[i] = mk<T>((y[i].x - am * yprev.x) * ibp, (y[i].y - am * yprev.y) * ibp);
@@ -231,7 +245,7 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
         for (int j = 0; j < K; ++j) {
             const C ys = sYs[j][lane], ye = sYe[j][lane];
             const T vs = sVs[j][lane], ws = sWs[j][lane], ve = sVe[j][lane], we = sWe[j][lane];
-            const T iden = (T)1 / ((T)1 - vs * Q);
+            const T iden = rcp_sweep<T>((T)1 - vs * Q);
             const C Sj = mk<T>((ys.x + vs * P.x) * iden, (ys.y + vs * P.y) * iden);
             const T Tj = ws * iden;
             const C Pj = mk<T>(ye.x + ve * (P.x + Q * Sj.x), ye.y + ve * (P.y + Q * Sj.y));
