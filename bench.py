@@ -208,6 +208,7 @@ def algorithmic_bytes(name, info, s):
         "tdma": 5 * lhx * ny * L * c,
         "tdma_mixed": 5 * lhx * ny * L * c,
         "tdma_reg": 5 * lhx * ny * L * c,
+        "tdma_staged": 5 * lhx * ny * L * c,
         # levels 1..L of H_x and 0..L+1 of H_z in, the y-transform of G over H_x out (2 launches)
         "press_gform_cols": ((L + (L + 2) + L) * lhx * ny * c) / 2,
         # one launch per field: field in, ddx and the x-padded rows out, and on u, v, w the

@@ -353,6 +353,18 @@ int obl_ensemble_last_error(const obl_ensemble *ens, char *buf, size_t n);
    up after a few seconds and OBL_ERR_TIMEOUT is returned, the context staying usable. */
 int obl_selftest_grid_barrier(obl_ctx *ctx, int never_released);
 
+/* Bounds-checked build (compiled with -DOBL_CHECK=1; no counterpart in the reference): the
+   hot-path kernels test each checked global index against the extents their arguments
+   give, record a failed test and skip the access instead of making it.  After the device
+   has drained, *count = the failed tests since the last call (the records are then
+   cleared) and buf (n > 0, may be NULL) describes the first: its check site and index.
+   *count = -1 in the product build, which has no checks. */
+int obl_check_report(long long *count, char *buf, size_t n);
+/* Bounds-checked build: one thread fails one check (index 1 against an extent of 1, with no
+   access made), so that obl_check_report then gives count 1 at site 12; the record path
+   is tested without a wrong index in a kernel.  OBL_ERR_UNSUPPORTED in the product build. */
+int obl_check_selftest(void);
+
 /* ---- the step on a z-slab of a domain split over nranks ranks (one GPU each) ----
    The reference splits z over npz MPI ranks and pipelines its Thomas sweeps rank by rank
    with a send/recv per y-row (109_press_stag_array.f90:244-319, 103_flosol.f90:169-173).

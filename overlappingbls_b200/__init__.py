@@ -41,7 +41,8 @@ EXPORTS = [
     "obl_divstress_uv", "obl_divstress_w", "obl_divstress_uv_dev", "obl_divstress_w_dev",
     "obl_divstress_uv_slab_dev", "obl_divstress_w_slab_dev",
     "obl_write_file_3d_dev", "obl_read_file_3d_dev", "obl_checkpoint_final_dev", "obl_read_flow_field_dev",
-    "obl_read_total_time", "obl_write_total_time", "obl_selftest_grid_barrier",
+    "obl_read_total_time", "obl_write_total_time", "obl_selftest_grid_barrier", "obl_check_report",
+    "obl_check_selftest",
     "obl_fftn", "obl_ifftn", "obl_fftn_dev", "obl_ifftn_dev",
     "obl_zero_padding", "obl_zero_unpadding", "obl_zero_padding_dev", "obl_zero_unpadding_dev",
     "obl_zero_padding_noalloc_dev",
@@ -132,6 +133,8 @@ def load_library(path=LIB_PATH):
         "obl_read_total_time": [ctypes.c_char_p, ctypes.POINTER(I)],
         "obl_write_total_time": [ctypes.c_char_p, I],
         "obl_selftest_grid_barrier": [ctx, I],
+        "obl_check_report": [ctypes.POINTER(ctypes.c_longlong), ctypes.c_char_p, ctypes.c_size_t],
+        "obl_check_selftest": [],
         "obl_fftn": [ctx, P, P, I], "obl_ifftn": [ctx, P, P, I],
         "obl_fftn_dev": [ctx, P, P, I], "obl_ifftn_dev": [ctx, P, P, I],
         "obl_zero_padding": [ctx, P, P, I], "obl_zero_unpadding": [ctx, P, P, I],
@@ -567,6 +570,24 @@ def read_total_time(fn):
     if rc:
         raise OblError(f"read_total_time({fn}): {ERRORS.get(rc, rc)}")
     return n.value
+
+
+def check_report():
+    """(failed index checks since the last call, description of the first) of the
+    bounds-checked build (-DOBL_CHECK=1); (-1, "") with the product build."""
+    n = ctypes.c_longlong(0)
+    buf = ctypes.create_string_buffer(256)
+    rc = load_library().obl_check_report(ctypes.byref(n), buf, 256)
+    if rc:
+        raise OblError(f"check_report: {ERRORS.get(rc, rc)}")
+    return n.value, buf.value.decode()
+
+
+def check_selftest():
+    """Bounds-checked build: record one failed check (no access made); see check_report."""
+    rc = load_library().obl_check_selftest()
+    if rc:
+        raise OblError(f"check_selftest: {ERRORS.get(rc, rc)}")
 
 
 def write_total_time(fn, nums):

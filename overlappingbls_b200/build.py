@@ -1,11 +1,14 @@
 """Build libobl_b200.so (sm_100a) in-tree with nvcc.
 
     python -m overlappingbls_b200.build [--force] [-j N] [-D NAME=VALUE ...] [--out PATH] [--tuned [WORKLOAD]]
+                                        [--checked]
 
 Objects go to overlappingbls_b200/_build/ (git-ignored); the shared library is
 written next to this file so that it travels with the source tree.  -D passes
 compile-time tuning definitions (e.g. OBL_SIDX_SHIFT=4) and --out writes a variant
-library elsewhere (with its own object directory), loadable through $OBL_LIB.
+library elsewhere (with its own object directory under _build/), loadable through
+$OBL_LIB.  --checked writes the bounds-checked build libobl_b200_check.so
+(-DOBL_CHECK=1).
 """
 import argparse
 import concurrent.futures as cf
@@ -18,6 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libobl_b200.so")
+# the bounds-checked build (-DOBL_CHECK=1: index checks that record and skip, see csrc/check.cuh)
+LIB_CHECK = os.path.join(HERE, "libobl_b200_check.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -50,8 +55,8 @@ def _compile(src, force, hdr_mtime, build_dir=BUILD, defines=()):
 
 def build(force=False, jobs=None, verbose=False, defines=(), out=None):
     lib = out or LIB
-    build_dir = BUILD if out is None else os.path.join(os.path.dirname(os.path.abspath(out)), "_objs_" +
-                                                       os.path.basename(out).replace(".so", ""))
+    # a variant's objects (other definitions) go to their own folder under _build/
+    build_dir = BUILD if out is None else os.path.join(BUILD, os.path.basename(out).replace(".so", ""))
     os.makedirs(build_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdr = _deps()
@@ -81,10 +86,14 @@ if __name__ == "__main__":
     ap.add_argument("-j", type=int, default=None)
     ap.add_argument("-D", dest="defines", action="append", default=[])
     ap.add_argument("--out", default=None)
+    ap.add_argument("--checked", action="store_true", help="the bounds-checked build, libobl_b200_check.so")
     ap.add_argument("--tuned", nargs="?", const="512x512x256", default=None, metavar="WORKLOAD",
                     help="add the schedule the tuner's cache chose for WORKLOAD (overlappingbls_b200.tune)")
     a = ap.parse_args()
     defines = list(a.defines)
+    if a.checked:
+        defines.append("OBL_CHECK=1")
+        a.out = a.out or LIB_CHECK
     if a.tuned:
         from overlappingbls_b200 import tune
         defines += tune.tuned_defines(a.tuned)

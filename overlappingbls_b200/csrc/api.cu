@@ -60,6 +60,7 @@ struct obl_ctx {
     int *d_isl = nullptr;
     unsigned char *d_skip = nullptr;
     int *d_isl_slot = nullptr;   // column -> island index, -1 for the bulk (z-slab solve)
+    int *d_ctl = nullptr;        // {work counter, error flag} of the staged solve (persistent kernel)
     // work buffers
     DevBuf spec[5];            // Hx, Hy, Hz, phat, dpdz spectrum (lhx*nyt*(nz+1) complex)
     DevBuf cscr;               // c' scratch
@@ -85,6 +86,8 @@ struct obl_ctx {
     long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
+    long long param_tdma_stage = 1;     // the segmented solve fed by bulk asynchronous copies (1) or by loads (0)
+    long long param_stage_timeout_test = 0;   // 1: the staged solve's waits expect bytes that never arrive
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
     long long param_out_streams = 2;    // host step: device -> host copy streams (1 or 2)
     long long param_fwd_chunk = 0;      // forward pass in chunks of this many levels (0 = whole fields)
@@ -103,6 +106,19 @@ struct obl_ctx {
 };
 
 // ----------------------------------------------------------------------------- helpers
+namespace obl {
+// readers of the index-check records of the translation units (bounds-checked build)
+static std::vector<CheckReader> &check_readers()
+{
+    static std::vector<CheckReader> v;
+    return v;
+}
+int check_register(CheckReader r)
+{
+    check_readers().push_back(r);
+    return 0;
+}
+} // namespace obl
 static int fail(obl_ctx *c, int code, const std::string &m)
 {
     if (c) c->err = m;
@@ -111,6 +127,18 @@ static int fail(obl_ctx *c, int code, const std::string &m)
 static int cuda_fail(obl_ctx *c, cudaError_t e, const char *where)
 {
     return fail(c, OBL_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+// The error flag a bounded device-side wait raises (the staged pressure solve's wait for
+// its copies), read once the context's work has drained; reported as OBL_ERR_TIMEOUT.
+static int device_status(obl_ctx *c)
+{
+    if (!c->d_ctl) return OBL_OK;
+    int flag = 0;
+    const cudaError_t e = cudaMemcpy(&flag, c->d_ctl + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(c, e, "device status");
+    if (!flag) return OBL_OK;
+    cudaMemset(c->d_ctl + 1, 0, sizeof(int));
+    return fail(c, OBL_ERR_TIMEOUT, "pressure solve: a bounded wait for its staged copies gave up");
 }
 #define CK(call)                                                                                   \
     do {                                                                                           \
@@ -508,9 +536,15 @@ template <typename T> struct Ops {
                         if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
                         isl = IslandArgs{ctx->d_isl, ctx->n_isl, (double *)ctx->isl_c.p, (double2 *)ctx->isl_d.p};
                     }
-                    LaunchScope ls(ctx->rec, "tdma_reg", s());
-                    launch_tdma_reg<float>(ta, isl, s(), e);
-                    if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_reg");
+                    if (ctx->param_tdma_stage && tdma_staged_supported(ta)) {
+                        LaunchScope ls(ctx->rec, "tdma_staged", s());
+                        launch_tdma_staged(ta, isl, ctx->d_ctl, ctx->param_stage_timeout_test ? 16u : 0u, s(), e);
+                        if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_staged");
+                    } else {
+                        LaunchScope ls(ctx->rec, "tdma_reg", s());
+                        launch_tdma_reg<float>(ta, isl, s(), e);
+                        if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_reg");
+                    }
                     done = true;
                 }
             }
@@ -1312,7 +1346,7 @@ template <typename HT, class F> static int host_call(obl_ctx *ctx, std::vector<H
             CK(cudaMemcpy2DAsync(hdst, hb * a.ld, dsrc, hb * a.ld, hb * a.width, a.nrows, cudaMemcpyDeviceToHost, s));
     }
     CK(cudaStreamSynchronize(s));
-    return OBL_OK;
+    return device_status(ctx);
 }
 
 } // namespace
@@ -1385,6 +1419,8 @@ int obl_ctx_create(const obl_grid *grid, const obl_options *opt, obl_ctx **out)
         return cudaMemcpy(*d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
     };
     if (!upload(&ctx->d_kx, kx) || !upload(&ctx->d_ky1, ky1) || !upload(&ctx->d_ky2, ky2)) return bad(OBL_ERR_NOMEM);
+    if (dev_malloc(ctx, (void **)&ctx->d_ctl, 4 * sizeof(int)) != cudaSuccess) return bad(OBL_ERR_NOMEM);
+    if (cudaMemset(ctx->d_ctl, 0, 4 * sizeof(int)) != cudaSuccess) return bad(OBL_ERR_CUDA);
 
     // plan twiddle tables (FP64 on the host, stored in the storage precision) for the
     // forward / backward / padded transforms of both horizontal lengths
@@ -1475,6 +1511,7 @@ int obl_ctx_destroy(obl_ctx *ctx)
     cudaFree(ctx->slab_iv.p);
     cudaFree(ctx->slab_icp.p);
     cudaFree(ctx->d_isl_slot);
+    cudaFree(ctx->d_ctl);
     for (auto &b : ctx->stage) cudaFree(b.p);
     for (auto &b : ctx->stage64) cudaFree(b.p);
     if (ctx->cin) cudaStreamDestroy(ctx->cin);
@@ -1510,7 +1547,7 @@ int obl_synchronize(obl_ctx *ctx)
 {
     CTX_OK();
     CK(cudaStreamSynchronize(ctx->stream));
-    return OBL_OK;
+    return device_status(ctx);
 }
 
 int obl_last_error(const obl_ctx *ctx, char *buf, size_t n)
@@ -1531,6 +1568,8 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "tdma_segments")) return &ctx->param_tdma_segments;
     if (!std::strcmp(name, "fail_alloc")) return &ctx->param_fail_alloc;
     if (!std::strcmp(name, "tdma_reg")) return &ctx->param_tdma_reg;
+    if (!std::strcmp(name, "tdma_stage")) return &ctx->param_tdma_stage;
+    if (!std::strcmp(name, "stage_timeout_test")) return &ctx->param_stage_timeout_test;
     if (!std::strcmp(name, "gform")) return &ctx->param_gform;
     if (!std::strcmp(name, "out_streams")) return &ctx->param_out_streams;
     if (!std::strcmp(name, "fwd_chunk")) return &ctx->param_fwd_chunk;
@@ -1687,6 +1726,39 @@ int obl_ddz_uv_dev(obl_ctx *ctx, void *dfdz, const void *fun)
 {
     if (!ctx || !dfdz || !fun) return OBL_ERR_ARG;
     DEVCALL(ctx, return o.ddz_uv((T *)dfdz, (const T *)fun););
+}
+#if OBL_CHECK
+__global__ void k_check_selftest() { ck_in(1, 1, CK_SELFTEST); }
+#endif
+int obl_check_selftest(void)
+{
+#if OBL_CHECK
+    k_check_selftest<<<1, 1>>>();
+    return cudaDeviceSynchronize() == cudaSuccess ? OBL_OK : OBL_ERR_CUDA;
+#else
+    return OBL_ERR_UNSUPPORTED;
+#endif
+}
+int obl_check_report(long long *count, char *buf, size_t n)
+{
+    if (!count) return OBL_ERR_ARG;
+    if (buf && n) buf[0] = 0;
+#if OBL_CHECK
+    if (cudaDeviceSynchronize() != cudaSuccess) return OBL_ERR_CUDA;
+    unsigned long long total = 0, first = 0;
+    for (CheckReader r : check_readers()) {
+        CheckRecord rec{0, 0};
+        r(&rec, true);
+        total += rec.count;
+        if (!first && rec.first) first = rec.first;
+    }
+    *count = (long long)total;
+    if (buf && n && total)
+        std::snprintf(buf, n, "check site %d, index %lld", (int)(first >> 48), (long long)(first & 0xffffffffffffULL));
+#else
+    *count = -1;
+#endif
+    return OBL_OK;
 }
 int obl_selftest_grid_barrier(obl_ctx *ctx, int never_released)
 {
@@ -2160,7 +2232,7 @@ template <typename HT, typename T> static int step_host_overlapped(obl_ctx *ctx,
     for (int i = 0; i < 3; ++i) CK(out(i, nf, nf, 0, 1));
     for (cudaStream_t co : cos) CK(cudaStreamSynchronize(co));
     CK(cudaStreamSynchronize(s));
-    return OBL_OK;
+    return device_status(ctx);
 }
 
 template <typename HT> static int step_host_any(obl_ctx *ctx, const obl_step_io *io)

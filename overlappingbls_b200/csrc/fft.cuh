@@ -12,6 +12,8 @@
 #include <type_traits>
 #include <utility>
 
+#include "check.cuh"
+
 namespace obl {
 
 // Kernel launchers cache one-time set-up (function attributes, occupancy-derived grid

@@ -291,7 +291,12 @@ __device__ __forceinline__ void rows_fwd3_unit(const RowsFwd3Args<T> &a, long lo
         const long long r0 = 2 * (act ? p : base);
         // warp-uniform: the LPW pairs of a warp lie on one level (ny/2 is a multiple of LPW)
         const int zw = a.z0 + (int)((2 * base) / a.ny);
-        const bool spec = a.H != nullptr && zw >= 1 && zw <= a.L;
+        bool spec = a.H != nullptr && zw >= 1 && zw <= a.L;
+        // checked build: the pair lies in the launch's rows, on one level, and its RHS rows
+        // in H's levels z0..L
+        if (OBL_CHECK && !(ck_in(r0 + 1, 2 * a.npairs, CK_ROWS3_ROW) && ck_in(r0 % a.ny + 1, a.ny, CK_ROWS3_ROW)))
+            return;
+        if (OBL_CHECK && spec && !ck_in(r0 + 1, (long long)(a.L + 1 - a.z0) * a.ny, CK_ROWS3_SPEC)) spec = false;
         const T *A = a.src + r0 * a.ldx;
         T *dA = a.dfdx + r0 * a.ldx;
         T *pA = a.xpad + r0 * N2;
@@ -362,8 +367,10 @@ __device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, 
 #pragma unroll
             for (int r = 0; r < R0; ++r) {
                 const int i = j + r * G0::NB;
-                v[b * R0 + r] = (act && (G0::FULL || j < G0::NB)) ? __ldcg(src + a.S * z + (long long)i * a.lhx + glc)
-                                                                   : mk<T>(0, 0);
+                v[b * R0 + r] = (act && (G0::FULL || j < G0::NB) &&
+                                 ck_in((long long)i * a.lhx + glc, a.S, CK_PINV_COL_LOAD))
+                                    ? __ldcg(src + a.S * z + (long long)i * a.lhx + glc)
+                                    : mk<T>(0, 0);
             }
         }
     };
@@ -374,7 +381,9 @@ __device__ __forceinline__ void pinv_cols_unit(const PinvColArgs<T> &a, int bx, 
             const int j = t + LL * b;
             if (GL::FULL || j < GL::NB)
 #pragma unroll
-                for (int r = 0; r < RL; ++r) dst[a.S * z + (long long)(j + r * GL::NB) * a.lhx + gl] = v[b * RL + r];
+                for (int r = 0; r < RL; ++r)
+                    if (ck_in((long long)(j + r * GL::NB) * a.lhx + gl, a.S, CK_PINV_COL_STORE))
+                        dst[a.S * z + (long long)(j + r * GL::NB) * a.lhx + gl] = v[b * RL + r];
         }
     };
     C v[VR], w[VR];
@@ -466,6 +475,9 @@ __device__ __forceinline__ void pinv_rows_unit(const PinvRowArgs<T> &a, long lon
         const long long r0 = 2 * (act ? pr : base);
         const int z = (int)((2 * base) / a.ny);            // warp-uniform level
         if (q > 0 && z == 0) return;                       // level 0 holds p only
+        // checked build: the pair lies in the launch's rows and on one level
+        if (OBL_CHECK && !(ck_in(r0 + 1, 2 * a.npairs, CK_PINV_ROW) && ck_in(r0 % a.ny + 1, a.ny, CK_PINV_ROW)))
+            return;
         const long long off = (r0 % a.ny) * a.ldx;
         const C *X = q <= 1 ? a.Xp : q == 2 ? a.Xdy : a.Xdz;
         T *out = q == 0 ? a.p + pl * z + off : (q == 1 ? a.dpdx : q == 2 ? a.dpdy : a.dpdz) + pl * (z - 1) + off;

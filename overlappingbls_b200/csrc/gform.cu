@@ -27,6 +27,7 @@ template <typename T, bool FIRST> struct GSrc {
     {
         const long long lv = lv0 + z;
         const long long q = (long long)i * lhx + gl;
+        if (!ck_in(q, S, CK_GFORM_LOAD)) return mk<T>(0, 0);
         const C2<T> hx = __ldcg(Hx + S * lv + q), hzc = __ldcg(Hz + S * lv + q), hzn = __ldcg(Hz + S * (lv + 1) + q);
         C2<T> dh = csub(hzn, hzc);
         if constexpr (FIRST) dh = cadd(dh, __ldcg(Hz + q));

@@ -611,13 +611,23 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
     // element i of this line: a complex value (a real column pair for REAL)
     const E *srcz = reinterpret_cast<const E *>(a.src) + (long long)z * a.src_plane;
     E *dstz = reinterpret_cast<E *>(a.dst) + (long long)z * a.dst_plane;
+    // the checked build tests each element's level, column and plane offset against the
+    // extents the arguments give (nlev planes of src_plane / dst_plane, rows of src_row / dst_row)
+    auto col_ok = [&](int i, int col, int row, long long plane, int site) {
+        const int ce = REAL ? 2 * col + 1 : col;
+        return ck_in(z, a.nlev, site) && ck_in(ce, row, site) && ck_in((long long)i * row + ce, plane, site);
+    };
     auto gld = [&](int i) -> C {
         if constexpr (!std::is_same<SRC, NoColSrc>::value) return src(z, i, glc);
         else if constexpr (SMEM_IN) return tile[i * WB + line];
-        else if constexpr (REAL) return __ldcg(reinterpret_cast<const C *>(srcz + (long long)i * a.src_row + 2 * glc));
-        else return __ldcg(srcz + (long long)i * a.src_row + glc);
+        else {
+            if (OBL_CHECK && !col_ok(i, glc, a.src_row, a.src_plane, CK_COL_LOAD)) return mk<T>(0, 0);
+            if constexpr (REAL) return __ldcg(reinterpret_cast<const C *>(srcz + (long long)i * a.src_row + 2 * glc));
+            else return __ldcg(srcz + (long long)i * a.src_row + glc);
+        }
     };
     auto gst = [&](int i, C v) {
+        if (OBL_CHECK && !col_ok(i, gl, a.dst_row, a.dst_plane, CK_COL_STORE)) return;
         if constexpr (REAL) *reinterpret_cast<C *>(dstz + (long long)i * a.dst_row + 2 * gl) = v;
         else dstz[(long long)i * a.dst_row + gl] = v;
     };
@@ -738,7 +748,7 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
                         gst(i, x);
                         if constexpr (OP == OP_UNPAD && REAL) {
                             // var(nxt+1:ldx,:) = var(1:2,:) (108_01_padd.f90:195)
-                            if (a.pad_copy && gl == 0)
+                            if (a.pad_copy && gl == 0 && ck_in(a.ncols + 1, a.dst_row, CK_COL_STORE))
                                 *reinterpret_cast<C *>(dstz + (long long)i * a.dst_row + a.ncols) = x;
                         }
                     }

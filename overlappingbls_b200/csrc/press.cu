@@ -13,6 +13,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "fft.cuh"
 #include "press.cuh"
 
 namespace obl {
@@ -95,184 +96,158 @@ template <typename T> __device__ __forceinline__ T rcp_sweep(T x)
 }
 constexpr int kRegLev = 16;      // rows a segment keeps in registers (so L <= 256)
 
-// NSEG segments (warps) per column; 16 / NSEG CTAs per SM, so fewer levels run with
-// smaller CTAs that overlap one another's load, solve and store phases
-template <typename T, int NSEG, bool G>
-__global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaArgs<T> a, IslandArgs isl, int nbi,
-                                                                          int Ls, int K)
+// Boundary coefficients of every segment (x_s = Ys + Vs x_{s-1} + Ws x_{e+1}, the same for
+// x_e).  The reduced solve runs in place: the upward elimination (x_s^j = S_j + T_j
+// x_s^{j+1}, x_e^j = P_j + Q_j x_s^{j+1}) overwrites Ys, Ws, Ye, We of row j with S, T, P, Q
+// once it has read them, and the downward substitution overwrites Ys, Ye with the solved
+// x_s, x_e.
+template <typename T, int NSEG> struct SegShared {
+    C2<T> Ys[NSEG][32], Ye[NSEG][32];
+    T Vs[NSEG][32], Ve[NSEG][32], Ws[NSEG][32], We[NSEG][32];
+};
+
+// Per-lane column of a segmented unit: lane l owns column q0 + l.
+template <typename T> struct SegCol {
+    long long q;
+    bool act, nyq, m00;
+    T kx, ky, k2;
+    __device__ __forceinline__ void init(const TdmaArgs<T> &a, long long q0, int lane)
+    {
+        q = q0 + lane;
+        const bool inq = q < a.S;
+        // q < S, and S (one spectral plane) fits 32 bits: one 32-bit division
+        const int iy = inq ? (int)((unsigned)q / (unsigned)a.lhx) : 0, ix = inq ? (int)q - iy * a.lhx : 0;
+        nyq = inq && (ix == a.lhx - 1 || iy == a.nyt / 2);
+        const bool isl_col = inq && a.skip && a.skip[q];
+        act = inq && !nyq && !isl_col;
+        const double kxd = act ? a.kx[ix] : 0.0, kyd = act ? a.ky[iy] : 0.0;
+        const double k2d = kxd * kxd + kyd * kyd;   // 002_fft.f90:167
+        m00 = (k2d == 0.0);
+        kx = (T)kxd;
+        ky = (T)kyd;
+        k2 = (T)k2d;
+    }
+};
+
+// RHS of row iz from the spectra (109:203-225): i*(kx*H_x + ky*H_y) + dH_z/dz, H_z(0)
+// added at iz = 1; the (0,0) mode takes H_z itself; a solved top row (npz = 1 mode) is 0.
+// dH_z/dz as dH_z * (1/dz): a product instead of a division sequence per row (within 1 ulp
+// of the quotient; the FP64 island columns divide in tdma_column).
+template <typename T>
+__device__ __forceinline__ C2<T> seg_rhs(const SegCol<T> &c, int iz, int L, bool top_solved, T idz, C2<T> hx, C2<T> hy,
+                                         C2<T> hzl, C2<T> hzu, C2<T> hz0)
 {
-    constexpr int kRegSeg = NSEG;
+    const C2<T> sxy = mk<T>(c.kx * hx.x + c.ky * hy.x, c.kx * hx.y + c.ky * hy.y);
+    C2<T> dh = csub(hzu, hzl);
+    if (iz == 1) dh = cadd(dh, hz0);
+    C2<T> r = mk<T>(-sxy.y + dh.x * idz, sxy.x + dh.y * idz);
+    if (c.m00) r = (iz == 1) ? mk<T>(0, 0) : hzl;
+    if (iz == L && !top_solved) r = mk<T>(0, 0);
+    return r;
+}
+
+// Forward sweep of rows s..s+ns-1 with x_{s-1} left unknown (x_i = y'_i + v'_i x_{s-1} -
+// c'_i x_{i+1}), then the segment's two boundary rows in terms of x_{s-1} and x_{e+1},
+// stored for the reduced solve.  Bands of 109:4-63 (the Neumann top row :33-38, npz >= 2).
+template <typename T, int NSEG>
+__device__ __forceinline__ void seg_eliminate(const SegCol<T> &c, C2<T> (&y)[kRegLev], T (&cp)[kRegLev],
+                                              T (&vp)[kRegLev], int s, int ns, int L, bool top_solved, T idz,
+                                              T idz2, SegShared<T, NSEG> &sh, int k, int lane)
+{
+    T cprev = 0, vprev = 1;
+    C2<T> yprev = mk<T>(0, 0);
+#pragma unroll
+    for (int i = 0; i < kRegLev; ++i) {
+        if (i < ns) {
+            const int iz = s + i;
+            T am, bm, cm;
+            if (iz == L && !top_solved) {
+                am = 0; bm = 1; cm = 0;
+            } else if (!c.m00) {
+                const bool top = iz == L;
+                am = (iz == 1) ? (T)0 : idz2;
+                bm = (iz == 1 || top) ? -(c.k2 + idz2) : -(c.k2 + (T)2 * idz2);
+                cm = top ? (T)0 : idz2;
+            } else {
+                am = (iz == 1) ? (T)0 : -idz;
+                bm = idz;
+                cm = 0;
+            }
+            const T ibp = rcp_sweep<T>(bm - am * cprev);
+            cp[i] = cm * ibp;
+            vp[i] = -am * vprev * ibp;
+            y[i] = mk<T>((y[i].x - am * yprev.x) * ibp, (y[i].y - am * yprev.y) * ibp);
+            cprev = cp[i];
+            vprev = vp[i];
+            yprev = y[i];
+        }
+    }
+    C2<T> ys = y[0];
+    T vs = 0, ws = 0;
+#pragma unroll
+    for (int i = kRegLev - 1; i >= 0; --i) {
+        if (i == ns - 1) {
+            ys = y[i];
+            vs = vp[i];
+            ws = -cp[i];
+            sh.Ye[k][lane] = ys;
+            sh.Ve[k][lane] = vs;
+            sh.We[k][lane] = ws;
+        } else if (i < ns - 1) {
+            ys = mk<T>(y[i].x - cp[i] * ys.x, y[i].y - cp[i] * ys.y);
+            vs = vp[i] - cp[i] * vs;
+            ws = -cp[i] * ws;
+        }
+    }
+    sh.Ys[k][lane] = ys;
+    sh.Vs[k][lane] = vs;
+    sh.Ws[k][lane] = ws;
+}
+
+// Lane l's reduced system of column l: 2K boundary values, a 2x2-block chain eliminated
+// upward and substituted downward, in place.
+template <typename T, int NSEG> __device__ __forceinline__ void seg_reduced(SegShared<T, NSEG> &sh, int K, int lane)
+{
     using C = C2<T>;
-    if ((int)blockIdx.x < nbi) {
-        tdma_column<T, double, true, G>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
-        return;
+    C P = mk<T>(0, 0);
+    T Q = 0;
+    for (int j = 0; j < K; ++j) {
+        const C ys = sh.Ys[j][lane], ye = sh.Ye[j][lane];
+        const T vs = sh.Vs[j][lane], ws = sh.Ws[j][lane], ve = sh.Ve[j][lane], we = sh.We[j][lane];
+        const T iden = rcp_sweep<T>((T)1 - vs * Q);
+        const C Sj = mk<T>((ys.x + vs * P.x) * iden, (ys.y + vs * P.y) * iden);
+        const T Tj = ws * iden;
+        const C Pj = mk<T>(ye.x + ve * (P.x + Q * Sj.x), ye.y + ve * (P.y + Q * Sj.y));
+        const T Qj = ve * Q * Tj + we;
+        sh.Ys[j][lane] = Sj;
+        sh.Ws[j][lane] = Tj;
+        sh.Ye[j][lane] = Pj;
+        sh.We[j][lane] = Qj;
+        P = Pj;
+        Q = Qj;
     }
-    // boundary coefficients of every segment (x_s = Ys + Vs x_{s-1} + Ws x_{e+1}, same for
-    // x_e), the reduced elimination (x_s^j = S_j + T_j x_s^{j+1}, x_e^j = P_j + Q_j x_s^{j+1})
-    // and the solved boundary values
-    __shared__ C sYs[kRegSeg][32], sYe[kRegSeg][32], sS[kRegSeg][32], sP[kRegSeg][32];
-    __shared__ C sXs[kRegSeg][32], sXe[kRegSeg][32];
-    __shared__ T sVs[kRegSeg][32], sVe[kRegSeg][32], sWs[kRegSeg][32], sWe[kRegSeg][32];
-    __shared__ T sT[kRegSeg][32], sQ[kRegSeg][32];
-    const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
-    const long long S = a.S;
-    const int L = a.L;
-    const long long q = (long long)(blockIdx.x - nbi) * 32 + lane;
-    const bool inq = q < S;
-    const int ix = inq ? (int)(q % a.lhx) : 0, iy = inq ? (int)(q / a.lhx) : 0;
-    const bool nyq = inq && (ix == a.lhx - 1 || iy == a.nyt / 2);
-    const bool isl_col = inq && a.skip && a.skip[q];
-    const bool act = inq && !nyq && !isl_col;
-    const int s = 1 + k * Ls;                                   // first row of the segment
-    const int ns = k < K ? min(Ls, L - s + 1) : 0;              // its rows (0: idle warp)
-    C *ph = a.phat + q;
-    C *dph = a.dph ? a.dph + q : nullptr;
+    // the top segment has no x_{e+1} (c = 0 in its last row): x_s = S, x_e = P stay in place
+    C xs = sh.Ys[K - 1][lane];
+    for (int j = K - 2; j >= 0; --j) {
+        const T Tj = sh.Ws[j][lane], Qj = sh.We[j][lane];
+        const C Sj = sh.Ys[j][lane], Pj = sh.Ye[j][lane];
+        sh.Ye[j][lane] = mk<T>(Pj.x + Qj * xs.x, Pj.y + Qj * xs.y);
+        xs = mk<T>(Sj.x + Tj * xs.x, Sj.y + Tj * xs.y);
+        sh.Ys[j][lane] = xs;
+    }
+}
 
-    // Nyquist columns: p_hat = 0 at every level (:303-305)
-    if (nyq && ns > 0) {
-        for (int i = 0; i < ns; ++i) {
-            ph[S * (s + i)] = mk<T>(0, 0);
-            if (dph) dph[S * (s + i)] = mk<T>(0, 0);
-        }
-        if (k == 0) ph[0] = mk<T>(0, 0);
-    }
-
-    const double kxd = act ? a.kx[ix] : 0.0, kyd = act ? a.ky[iy] : 0.0;
-    const double k2d = kxd * kxd + kyd * kyd;   // 002_fft.f90:167
-    const bool m00 = (k2d == 0.0);
-    const T kx = (T)kxd, ky = (T)kyd, k2 = (T)k2d;
-    const T dz = (T)a.dz, idz = (T)(1.0 / a.dz), idz2 = (T)(1.0 / (a.dz * a.dz));
-    const bool top_solved = a.neumann_top;      // else row L is p_hat(L) = 0 (npz = 1 mode)
-
-    C y[kRegLev];
-    T cp[kRegLev], vp[kRegLev];
-    C hz0 = mk<T>(0, 0);
-    if (act && ns > 0) {
-        // right-hand sides of rows s..s+ns-1 (:203-225).  Every load is issued without a
-        // condition (levels past the segment clamp to level L+1 and are not used), so all
-        // of the segment's loads are in flight together.
-        const long long qc = q;
-        hz0 = a.Hz[qc];   // RHS_col(0) = H_z(0) (:209), used by segment 0
-        C hx[kRegLev], hy[kRegLev];
-#pragma unroll
-        for (int i = 0; i < kRegLev; ++i) {
-            const long long zz = min(s + i, L);
-            hx[i] = __ldcs(a.Hx + qc + S * zz);
-            hy[i] = __ldcs(a.Hy + qc + S * zz);
-        }
-        if constexpr (G) {
-            // G + i*ky*H_y; the (0,0) mode takes H_z's own (0,0) value (q = 0)
-#pragma unroll
-            for (int i = 0; i < kRegLev; ++i) {
-                const int iz = s + i;
-                C r = mk<T>(hx[i].x - ky * hy[i].y, hx[i].y + ky * hy[i].x);
-                if (m00) r = (iz == 1) ? mk<T>(0, 0) : a.Hz[S * min(iz, L + 1)];
-                if (iz == L && !top_solved) r = mk<T>(0, 0);
-                y[i] = r;
-            }
-        } else {
-            C hz[kRegLev + 1];
-#pragma unroll
-            for (int i = 0; i <= kRegLev; ++i) hz[i] = __ldcs(a.Hz + qc + S * min(s + i, L + 1));
-#pragma unroll
-            for (int i = 0; i < kRegLev; ++i) {
-                const int iz = s + i;
-                const C sxy = mk<T>(kx * hx[i].x + ky * hy[i].x, kx * hx[i].y + ky * hy[i].y);
-                C dh = csub(hz[i + 1], hz[i]);
-                if (iz == 1) dh = cadd(dh, hz0);
-                C r = mk<T>(-sxy.y + dh.x / dz, sxy.x + dh.y / dz);
-                if (m00) r = (iz == 1) ? mk<T>(0, 0) : hz[i];
-                if (iz == L && !top_solved) r = mk<T>(0, 0);
-                y[i] = r;
-            }
-        }
-        // forward sweep with x_{s-1} left unknown: x_i = y'_i + v'_i x_{s-1} - c'_i x_{i+1}
-        T cprev = 0, vprev = 1;
-        C yprev = mk<T>(0, 0);
-#pragma unroll
-        for (int i = 0; i < kRegLev; ++i) {
-            if (i < ns) {
-                const int iz = s + i;
-                T am, bm, cm;
-                if (iz == L && !top_solved) {
-                    am = 0; bm = 1; cm = 0;
-                } else if (!m00) {
-                    const bool top = iz == L;   // the Neumann top row (:33-38 with npz >= 2)
-                    am = (iz == 1) ? (T)0 : idz2;
-                    bm = (iz == 1 || top) ? -(k2 + idz2) : -(k2 + (T)2 * idz2);
-                    cm = top ? (T)0 : idz2;
-                } else {
-                    am = (iz == 1) ? (T)0 : -idz;
-                    bm = idz;
-                    cm = 0;
-                }
-                const T ibp = rcp_sweep<T>(bm - am * cprev);
-                cp[i] = cm * ibp;
-                vp[i] = -am * vprev * ibp;
-                y[i] = mk<T>((y[i].x - am * yprev.x) * ibp, (y[i].y - am * yprev.y) * ibp);
-                cprev = cp[i];
-                vprev = vp[i];
-                yprev = y[i];
-            }
-        }
-        // the segment's two boundary rows in terms of x_{s-1} and x_{e+1}
-        C ys = y[0];
-        T vs = 0, ws = 0;
-#pragma unroll
-        for (int i = kRegLev - 1; i >= 0; --i) {
-            if (i == ns - 1) {
-                ys = y[i];
-                vs = vp[i];
-                ws = -cp[i];
-                sYe[k][lane] = ys;
-                sVe[k][lane] = vs;
-                sWe[k][lane] = ws;
-            } else if (i < ns - 1) {
-                ys = mk<T>(y[i].x - cp[i] * ys.x, y[i].y - cp[i] * ys.y);
-                vs = vp[i] - cp[i] * vs;
-                ws = -cp[i] * ws;
-            }
-        }
-        sYs[k][lane] = ys;
-        sVs[k][lane] = vs;
-        sWs[k][lane] = ws;
-    }
-    __syncthreads();
-    if (k == 0 && act) {
-        // reduced system: x_e^{j-1} = P + Q x_s^j eliminated upward, then substituted down
-        C P = mk<T>(0, 0);
-        T Q = 0;
-        for (int j = 0; j < K; ++j) {
-            const C ys = sYs[j][lane], ye = sYe[j][lane];
-            const T vs = sVs[j][lane], ws = sWs[j][lane], ve = sVe[j][lane], we = sWe[j][lane];
-            const T iden = rcp_sweep<T>((T)1 - vs * Q);
-            const C Sj = mk<T>((ys.x + vs * P.x) * iden, (ys.y + vs * P.y) * iden);
-            const T Tj = ws * iden;
-            const C Pj = mk<T>(ye.x + ve * (P.x + Q * Sj.x), ye.y + ve * (P.y + Q * Sj.y));
-            const T Qj = ve * Q * Tj + we;
-            sS[j][lane] = Sj;
-            sT[j][lane] = Tj;
-            sP[j][lane] = Pj;
-            sQ[j][lane] = Qj;
-            P = Pj;
-            Q = Qj;
-        }
-        C xs = sS[K - 1][lane];          // the top segment has no x_{e+1} (c = 0 in its last row)
-        sXs[K - 1][lane] = xs;
-        sXe[K - 1][lane] = sP[K - 1][lane];
-        for (int j = K - 2; j >= 0; --j) {
-            const T Tj = sT[j][lane], Qj = sQ[j][lane];
-            const C Sj = sS[j][lane], Pj = sP[j][lane];
-            sXe[j][lane] = mk<T>(Pj.x + Qj * xs.x, Pj.y + Qj * xs.y);
-            xs = mk<T>(Sj.x + Tj * xs.x, Sj.y + Tj * xs.y);
-            sXs[j][lane] = xs;
-        }
-    }
-    __syncthreads();
-    if (!act || ns == 0) return;
-    const C xl = k > 0 ? sXe[k - 1][lane] : mk<T>(0, 0);
-    const C xr = k < K - 1 ? sXs[k + 1][lane] : mk<T>(0, 0);
-    const T rdz = (T)(1.0 / a.dz);
+// Back-substitution of rows s..s+ns-1 from the neighbours' solved boundary values xl =
+// x_{s-1}, xr = x_{e+1}; stores p_hat and the dpdz spectrum, and on segment 0 the Neumann
+// ghost level below the wall (:313-315).
+template <typename T>
+__device__ __forceinline__ void seg_backsub(const C2<T> (&y)[kRegLev], const T (&cp)[kRegLev], const T (&vp)[kRegLev],
+                                            C2<T> xl, C2<T> xr, int s, int ns, int k, int L, C2<T> *ph, C2<T> *dph,
+                                            long long S, T dz, T rdz, C2<T> hz0)
+{
+    using C = C2<T>;
+    // checked build: the segment's rows lie in 1..L
+    if (OBL_CHECK && !(ck_in(s - 1, L, CK_TDMA_STORE) && ck_in(s + ns - 1, L + 1, CK_TDMA_STORE))) return;
     C x = mk<T>(0, 0);
 #pragma unroll
     for (int i = kRegLev - 1; i >= 0; --i) {
@@ -289,11 +264,93 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
     if (k > 0) {
         if (dph) dph[S * s] = mk<T>((x.x - xl.x) * rdz, (x.y - xl.y) * rdz);
     } else {
-        // Neumann ghost level below the wall (:313-315)
         const C p0 = mk<T>(x.x - dz * hz0.x, x.y - dz * hz0.y);
         ph[0] = p0;
         if (dph) dph[S] = mk<T>((x.x - p0.x) / dz, (x.y - p0.y) / dz);
     }
+}
+
+// Nyquist columns: p_hat = 0 at every level (:303-305)
+template <typename T>
+__device__ __forceinline__ void seg_nyquist(C2<T> *ph, C2<T> *dph, long long S, int s, int ns, int k, int L)
+{
+    if (ns <= 0) return;   // idle warp
+    if (OBL_CHECK && !(ck_in(s - 1, L, CK_TDMA_STORE) && ck_in(s + ns - 1, L + 1, CK_TDMA_STORE))) return;
+    for (int i = 0; i < ns; ++i) {
+        ph[S * (s + i)] = mk<T>(0, 0);
+        if (dph) dph[S * (s + i)] = mk<T>(0, 0);
+    }
+    if (k == 0) ph[0] = mk<T>(0, 0);
+}
+
+// NSEG segments (warps) per column; 16 / NSEG CTAs per SM, so fewer levels run with
+// smaller CTAs that overlap one another's load, solve and store phases
+template <typename T, int NSEG, bool G>
+__global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaArgs<T> a, IslandArgs isl, int nbi,
+                                                                          int Ls, int K)
+{
+    using C = C2<T>;
+    if ((int)blockIdx.x < nbi) {
+        tdma_column<T, double, true, G>(a, isl, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+        return;
+    }
+    __shared__ SegShared<T, NSEG> sh;
+    const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+    const long long S = a.S;
+    const int L = a.L;
+    SegCol<T> c;
+    c.init(a, (long long)(blockIdx.x - nbi) * 32, lane);
+    const long long q = c.q;
+    const int s = 1 + k * Ls;                                   // first row of the segment
+    const int ns = k < K ? min(Ls, L - s + 1) : 0;              // its rows (0: idle warp)
+    C *ph = a.phat + q;
+    C *dph = a.dph ? a.dph + q : nullptr;
+    if (c.nyq) seg_nyquist<T>(ph, dph, S, s, ns, k, L);
+
+    const T dz = (T)a.dz, idz = (T)(1.0 / a.dz), idz2 = (T)(1.0 / (a.dz * a.dz));
+    const bool top_solved = a.neumann_top;      // else row L is p_hat(L) = 0 (npz = 1 mode)
+
+    C y[kRegLev];
+    T cp[kRegLev], vp[kRegLev];
+    C hz0 = mk<T>(0, 0);
+    if (c.act && ns > 0) {
+        // right-hand sides of rows s..s+ns-1.  Every load is issued without a condition
+        // (levels past the segment clamp to level L+1 and are not used), so all of the
+        // segment's loads are in flight together.
+        hz0 = a.Hz[q];   // RHS_col(0) = H_z(0) (:209), used by segment 0
+        C hx[kRegLev], hy[kRegLev];
+#pragma unroll
+        for (int i = 0; i < kRegLev; ++i) {
+            const long long zz = min(s + i, L);
+            hx[i] = __ldcs(a.Hx + q + S * zz);
+            hy[i] = __ldcs(a.Hy + q + S * zz);
+        }
+        if constexpr (G) {
+            // G + i*ky*H_y; the (0,0) mode takes H_z's own (0,0) value (q = 0)
+#pragma unroll
+            for (int i = 0; i < kRegLev; ++i) {
+                const int iz = s + i;
+                C r = mk<T>(hx[i].x - c.ky * hy[i].y, hx[i].y + c.ky * hy[i].x);
+                if (c.m00) r = (iz == 1) ? mk<T>(0, 0) : a.Hz[S * min(iz, L + 1)];
+                if (iz == L && !top_solved) r = mk<T>(0, 0);
+                y[i] = r;
+            }
+        } else {
+            C hz[kRegLev + 1];
+#pragma unroll
+            for (int i = 0; i <= kRegLev; ++i) hz[i] = __ldcs(a.Hz + q + S * min(s + i, L + 1));
+#pragma unroll
+            for (int i = 0; i < kRegLev; ++i) y[i] = seg_rhs<T>(c, s + i, L, top_solved, idz, hx[i], hy[i], hz[i], hz[i + 1], hz0);
+        }
+        seg_eliminate<T, NSEG>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
+    }
+    __syncthreads();
+    if (k == 0 && c.act) seg_reduced<T, NSEG>(sh, K, lane);
+    __syncthreads();
+    if (!c.act || ns == 0) return;
+    const C xl = k > 0 ? sh.Ye[k - 1][lane] : mk<T>(0, 0);
+    const C xr = k < K - 1 ? sh.Ys[k + 1][lane] : mk<T>(0, 0);
+    seg_backsub<T>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, (T)(1.0 / a.dz), hz0);
 }
 
 bool tdma_reg_supported(int L) { return L >= 1 && L <= kRegSegMax * kRegLev; }
@@ -320,6 +377,227 @@ void launch_tdma_reg(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s
     else launch_tdma_reg_n<T, 2>(a, isl, s, e);
 }
 template void launch_tdma_reg<float>(const TdmaArgs<float> &, const IslandArgs &, cudaStream_t, cudaError_t &);
+
+// ----------------------------------------------------------------------------- staged segmented solve
+// The register-segmented solve as a persistent kernel whose RHS rows arrive by bulk
+// asynchronous copies.  k_tdma_reg runs one 512-thread CTA per SM at 256 levels (128
+// registers a thread), so its load, eliminate, reduced-solve and store phases follow one
+// another and HBM idles while the SM computes.  Here each CTA walks units taken from a
+// work counter (FP64 island units first, then 32-column groups) and, as soon as a warp has
+// read its segment's rows of the current group out of shared memory, it starts the copies
+// of the next group's rows into the same buffer: one cp.async.bulk per level and spectrum
+// (256 contiguous bytes), completing on the warp's mbarrier.  The copies of group g+1 are
+// in flight while group g is eliminated, reduced, back-substituted and stored.
+//
+// Buffer of warp k: kStageRows rows of 32 columns, H_x and H_y at levels s..s+15 and H_z
+// at s..s+16 (levels past the segment clamp to L and L+1, as in k_tdma_reg).  Copies need
+// 16-byte aligned addresses and sizes: the host launches this kernel only when S is even
+// and the spectra are 16-byte aligned (a group's first column is then 256-byte aligned in
+// every plane and a ragged last group copies an even number of 8-byte columns).
+//
+// Every wait is bounded: a warp whose copies have not landed after kStageWaitNs raises the
+// error flag ctl[1] (the host reports OBL_ERR_TIMEOUT) and the CTA stops after the unit,
+// waiting (bounded again) for the copies it still has in flight.  extra_tx (0 in the
+// product path) is added to the bytes each wait expects: bytes no copy delivers, so that a
+// test can make the waits run out and check the reported status.
+constexpr int kStageRows = 3 * kRegLev + 1;
+constexpr unsigned long long kStageWaitNs = 1000000000ULL;
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// true once the phase of the given parity has completed; false after kStageWaitNs
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kStageWaitNs) return false;
+    return true;
+}
+
+template <int NSEG>
+__global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_staged(TdmaArgs<float> a, IslandArgs isl, int nbi, int Ls,
+                                                              int K, int *ctl, unsigned extra_tx)
+{
+    using T = float;
+    using C = C2<T>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ SegShared<T, NSEG> sh;
+    __shared__ __align__(8) unsigned long long sBar[NSEG];
+    __shared__ int sUnit[3];   // [it & 1]: the unit after next, fetched during unit it; [2]: grab()
+    __shared__ int sAbort;
+    const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+    const long long S = a.S;
+    const int L = a.L;
+    const long long nunits = nbi + (S + 31) / 32;
+    const int s = 1 + k * Ls;
+    const int ns = k < K ? min(Ls, L - s + 1) : 0;
+    C *buf = reinterpret_cast<C *>(smraw) + (size_t)k * kStageRows * 32;
+    const unsigned bar = smem_addr(&sBar[k]);
+    const T dz = (T)a.dz, idz = (T)(1.0 / a.dz), idz2 = (T)(1.0 / (a.dz * a.dz)), rdz = idz;
+    const bool top_solved = a.neumann_top;
+
+    if (lane == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    if (threadIdx.x == 0) sAbort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n\tfence.proxy.async.shared::cta;" ::: "memory");
+    auto grab = [&]() -> long long {
+        __syncthreads();
+        if (threadIdx.x == 0) sUnit[2] = atomicAdd(ctl, 1);
+        __syncthreads();
+        return sUnit[2];
+    };
+
+    // FP64 island units (the counter hands them out first): their sequential sweeps
+    long long cur = grab();
+    while (cur < nbi) {
+        tdma_column<T, double, true, false>(a, isl, cur * blockDim.x + threadIdx.x);
+        cur = grab();
+    }
+    if (cur >= nunits) return;
+    long long nxt = grab();
+
+    // copies of this warp's rows of group unit u into its buffer (after its reads of the
+    // buffer: the proxy fence orders them before the async writes)
+    auto issue = [&](long long u) {
+        const long long q0 = (u - nbi) * 32;
+        const unsigned rb = (unsigned)(8 * (S - q0 < 32 ? S - q0 : 32));
+        // checked build: the group's columns lie in the plane (a skipped copy leaves the
+        // wait to give up, which the host reports as well)
+        if (OBL_CHECK && !(ck_in(q0, S, CK_TDMA_COPY) && ck_in(q0 + rb / 8 - 1, S, CK_TDMA_COPY))) return;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(rb * kStageRows + extra_tx)
+                         : "memory");
+        __syncwarp();
+        for (int r = lane; r < kStageRows; r += 32) {
+            const C *src = r < kRegLev       ? a.Hx + S * min(s + r, L)
+                           : r < 2 * kRegLev ? a.Hy + S * min(s + r - kRegLev, L)
+                                             : a.Hz + S * min(s + r - 2 * kRegLev, L + 1);
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_addr(buf + r * 32)),
+                         "l"(src + q0), "r"(rb), "r"(bar)
+                         : "memory");
+        }
+    };
+
+    unsigned parity = 0;
+    bool pending = false;   // this warp has copies in flight
+    if (ns > 0) {
+        issue(cur);
+        pending = true;
+    }
+    for (int it = 0; cur < nunits; ++it) {
+        if (threadIdx.x == 0) sUnit[it & 1] = atomicAdd(ctl, 1);
+        const bool nxt_bulk = nxt < nunits;   // the counter only grows: nxt > cur >= nbi
+        {
+            SegCol<T> c;
+            c.init(a, (cur - nbi) * 32, lane);
+            const long long q = c.q;
+            C *ph = a.phat + q;
+            C *dph = a.dph ? a.dph + q : nullptr;
+            const C hz0 = (k == 0 && c.act) ? a.Hz[q] : mk<T>(0, 0);
+            C y[kRegLev];
+            T cp[kRegLev], vp[kRegLev];
+            if (ns > 0) {
+                // warp-uniform outcome; after a timeout the phase stays pending (its copies
+                // may still land) and no further copies are started
+                const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
+                if (ok) {
+                    parity ^= 1;
+                    pending = false;
+                } else if (lane == 0) {
+                    atomicExch(ctl + 1, 1);
+                    sAbort = 1;
+                }
+                if (c.act) {
+#pragma unroll
+                    for (int i = 0; i < kRegLev; ++i)
+                        y[i] = seg_rhs<T>(c, s + i, L, top_solved, idz, buf[i * 32 + lane], buf[(kRegLev + i) * 32 + lane],
+                                          buf[(2 * kRegLev + i) * 32 + lane], buf[(2 * kRegLev + i + 1) * 32 + lane], hz0);
+                }
+                if (nxt_bulk && ok) {
+                    issue(nxt);
+                    pending = true;
+                }
+                if (c.nyq) seg_nyquist<T>(ph, dph, S, s, ns, k, L);
+                if (c.act) seg_eliminate<T, NSEG>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
+            }
+            __syncthreads();
+            if (k == 0 && c.act) seg_reduced<T, NSEG>(sh, K, lane);
+            __syncthreads();
+            const C xl = k > 0 ? sh.Ye[k - 1][lane] : mk<T>(0, 0);
+            const C xr = k < K - 1 ? sh.Ys[k + 1][lane] : mk<T>(0, 0);
+            __syncthreads();   // the next unit's boundary rows overwrite sh
+            if (c.act && ns > 0) seg_backsub<T>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, rdz, hz0);
+        }
+        cur = nxt;
+        nxt = sUnit[it & 1];
+        if (sAbort) break;
+    }
+    // copies still in flight (a stop after a timed-out wait) land before the CTA exits
+    if (pending) mbar_wait_bounded(bar, parity);
+}
+
+bool tdma_staged_supported(const TdmaArgs<float> &a)
+{
+    const auto al = [](const void *p) { return ((uintptr_t)p % 16) == 0; };
+    return tdma_reg_supported(a.L) && !a.gform && a.S % 2 == 0 && al(a.Hx) && al(a.Hy) && al(a.Hz);
+}
+
+template <int NSEG>
+static void launch_tdma_staged_n(const TdmaArgs<float> &a, const IslandArgs &isl, int *ctl, unsigned extra_tx,
+                                 cudaStream_t s, cudaError_t &e)
+{
+    constexpr int bs = 32 * NSEG;
+    const size_t smem = sizeof(C2<float>) * (size_t)NSEG * kStageRows * 32;
+    static int residents[kMaxDevices] = {};   // CTAs resident on the whole GPU
+    const int ds = device_slot();
+    int resident = ds >= 0 ? residents[ds] : 0;
+    if (!resident) {
+        e = cudaFuncSetAttribute(k_tdma_staged<NSEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return;
+        int dev = 0, nsm = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tdma_staged<NSEG>, bs, smem);
+        resident = nsm * (per > 0 ? per : 1);
+        if (ds >= 0) residents[ds] = resident;
+    }
+    const int Ls = (a.L + NSEG - 1) / NSEG, K = (a.L + Ls - 1) / Ls;
+    const int nbi = (int)((isl.n + bs - 1) / bs);
+    const long long nunits = nbi + (a.S + 31) / 32;
+    const int grid = (int)(nunits < resident ? nunits : resident);
+    if (grid < 1) return;
+    e = cudaMemsetAsync(ctl, 0, sizeof(int), s);   // the work counter
+    if (e != cudaSuccess) return;
+    k_tdma_staged<NSEG><<<grid, bs, smem, s>>>(a, isl, nbi, Ls, K, ctl, extra_tx);
+    e = cudaGetLastError();
+}
+
+void launch_tdma_staged(const TdmaArgs<float> &a, const IslandArgs &isl, int *ctl, unsigned extra_tx, cudaStream_t s,
+                        cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    if (a.L > 8 * kRegLev) launch_tdma_staged_n<16>(a, isl, ctl, extra_tx, s, e);
+    else if (a.L > 4 * kRegLev) launch_tdma_staged_n<8>(a, isl, ctl, extra_tx, s, e);
+    else if (a.L > 2 * kRegLev) launch_tdma_staged_n<4>(a, isl, ctl, extra_tx, s, e);
+    else launch_tdma_staged_n<2>(a, isl, ctl, extra_tx, s, e);
+}
 
 // ----------------------------------------------------------------------------- streaming
 // The level kernels run over (level, x-vector, y) with VW consecutive x per access (2

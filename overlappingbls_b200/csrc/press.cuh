@@ -214,6 +214,12 @@ cudaError_t launch_gform_cols(int ny, C2<T> *Hx, const C2<T> *Hz, const double *
 // FP64 island columns (isl.n may be 0) by the sequential FP64 sweep in the same launch;
 // levels L <= 256
 bool tdma_reg_supported(int L);
+// the same solve as a persistent kernel fed by bulk asynchronous copies (FP32 storage, the
+// three-spectra RHS); ctl: device ints {work counter, error flag}, the flag set to 1 when a
+// bounded wait gave up; extra_tx: 0 (a test sets bytes that never arrive)
+bool tdma_staged_supported(const TdmaArgs<float> &a);
+void launch_tdma_staged(const TdmaArgs<float> &a, const IslandArgs &isl, int *ctl, unsigned extra_tx, cudaStream_t s,
+                        cudaError_t &e);
 template <typename T> void launch_tdma_reg(const TdmaArgs<T> &a, const IslandArgs &isl, cudaStream_t s,
                                            cudaError_t &e);
 template <typename T> void launch_tdma_island(const TdmaArgs<T> &a, const IslandArgs &isl,

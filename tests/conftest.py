@@ -36,6 +36,20 @@ def pytest_collection_modifyitems(config, items):
             it.add_marker(skip)
 
 
+@pytest.fixture(autouse=True)
+def _index_checks(request):
+    """Under the bounds-checked build (tests/test_gpu_checked.py runs a subset of the GPU
+    tests with $OBL_LIB = libobl_b200_check.so and $OBL_CHECKED_RUN = 1), every GPU test
+    must leave no failed index check behind."""
+    yield
+    if os.environ.get("OBL_CHECKED_RUN") != "1" or "gpu" not in request.keywords:
+        return
+    import overlappingbls_b200 as obl
+    n, first = obl.check_report()
+    assert n != -1, "OBL_CHECKED_RUN is set but the loaded library has no index checks"
+    assert n == 0, f"{n} failed index checks, the first: {first}"
+
+
 @pytest.fixture(scope="session")
 def orc():
     from oracle import orc as _orc

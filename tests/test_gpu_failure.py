@@ -94,3 +94,39 @@ def test_entry_point_allocation_failure_then_recovery(orc, which):
     # the context is still usable and the answer is right
     assert call() < 1e-12, name
     ctx.close()
+
+
+def test_staged_solve_wait_gives_up(orc):
+    """The staged pressure solve waits for its bulk copies on mbarriers with a bound of
+    about a second.  With bytes expected that no copy delivers (the `stage_timeout_test`
+    parameter), every wait gives up, the step returns OBL_ERR_TIMEOUT when it synchronizes,
+    and the context then steps correctly again."""
+    import time
+    nx, ny, nzt = 64, 64, 65
+    L = nzt - 2
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
+    f = fields.make_fields(nx, ny, nzt)
+    ctx = obl.Context(nx, ny, nzt, precision="mixed", **fields.DOMAIN)
+    ctx.set_param("tdma_segments", 1)   # the whole-column solve (few columns pick the column-segmented one)
+
+    def step():
+        u, v, w = (f[k].copy(order="F") for k in "uvw")
+        d = [ctx.field() for _ in range(8)]
+        big = [ctx.big_field() for _ in range(4)]
+        p, dp = ctx.field(), [ctx.dfield() for _ in range(3)]
+        ctx.step(u, v, w, f["theta"], d, big, p, dp)
+        return p, w
+
+    ctx.set_param("stage_timeout_test", 1)
+    t0 = time.perf_counter()
+    with pytest.raises(obl.OblError, match="OBL_ERR_TIMEOUT"):
+        step()
+    waited = time.perf_counter() - t0
+    assert waited < 30.0
+    ctx.set_param("stage_timeout_test", 0)
+    p, w = step()
+    ref = g.step(f["u"], f["v"], f["w"], f["theta"], npz=2)
+    assert rel_l2(p[:nx, :, :L + 1], ref["p"][:nx, :, :L + 1]) < 1e-5
+    assert rel_l2(w, ref["w"]) < 1e-5
+    print(f"staged solve: the waits gave up and the step returned after {waited:.1f} s")
+    ctx.close()

@@ -192,22 +192,34 @@ def test_headline_size_step_is_divergence_free(prec):
 @pytest.mark.parametrize("nx,ny,nzt", [(512, 256, 9), (256, 256, 34), (256, 512, 129), (512, 256, 257)])
 def test_register_segmented_solve(orc, prec, top, nx, ny, nzt):
     """The FP32 columns' register-segmented partitioned solve (16 segments of up to 16 rows
-    per column, reduced system in shared memory) against the one-sweep solve it replaces and
-    against the oracle: 8 rows (one row per segment), 33 rows (ragged segments), 128 and 256
-    rows; both top modes, with divtz boundary planes; FP64 islands (mixed) or none (f32)."""
+    per column, reduced system in shared memory), in its persistent form fed by bulk
+    asynchronous copies (`staged`, the default) and in its load-fed form (`reg`), against
+    the one-sweep solve they replace (`sweep`) and against the oracle: 8 rows (one row per
+    segment), 33 rows (ragged segments), 128 and 256 rows; both top modes, with divtz
+    boundary planes; FP64 islands (mixed) or none (f32)."""
     ctx = obl.Context(nx, ny, nzt, precision=prec, top_bc=top, **fields.DOMAIN)
+    ctx.set_param("tdma_segments", 1)   # whole columns (grids of few columns pick the column-segmented solve)
     f = identical_inputs(fields.make_fields(nx, ny, nzt), "mixed")
     rng = np.random.default_rng(3)
     pl = identical_inputs({k: np.asfortranarray(0.1 * rng.standard_normal((ctx.ldx, ny))) for k in ("b", "t")},
                           "mixed")
     L = ctx.nz - 1
     outs = {}
-    for reg in (1, 0):
+    for name, reg, stage in (("staged", 1, 1), ("reg", 1, 0), ("sweep", 0, 0)):
         ctx.set_param("tdma_reg", reg)
+        ctx.set_param("tdma_stage", stage)
         u, v, w = (f[k].copy(order="F") for k in "uvw")
         d, big, p, dp = _alloc_step(ctx)
         ctx.step(u, v, w, f["theta"], d, big, p, dp, pl["b"], pl["t"])
-        outs[reg] = (p, dp, u, v, w)
+        outs[name] = (p, dp, u, v, w)
+    # the staged and load-fed forms run the same arithmetic on the same values (the
+    # compiler may contract their products differently, hence a bound instead of equality)
+    flat = lambda o: [o[0], *o[1], *o[2:]]
+    same = all(np.array_equal(a, b) for a, b in zip(flat(outs["staged"]), flat(outs["reg"])))
+    print(f"staged vs load-fed solve bitwise equal: {same}")
+    for a, b in zip(flat(outs["staged"]), flat(outs["reg"])):
+        assert rel_l2(a, b) < 1e-6
+    outs = {1: outs["reg"], 0: outs["sweep"]}
     g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
     npz = 1 if top == "single" else (2 if L % 2 == 0 else 3)   # the oracle's ranks need whole levels
     rp, rdx, rdy = g.press_stag_array(f["u"], f["v"], f["w"], pl["b"], pl["t"], npz=npz)
