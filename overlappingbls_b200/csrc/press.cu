@@ -133,35 +133,42 @@ template <typename T> struct SegCol {
 // added at iz = 1; the (0,0) mode takes H_z itself; a solved top row (npz = 1 mode) is 0.
 // dH_z/dz as dH_z * (1/dz): a product instead of a division sequence per row (within 1 ulp
 // of the quotient; the FP64 island columns divide in tdma_column).
-template <typename T>
+// IN: a full segment away from both ends (rows 2..L-1 only), whose rows need no end cases.
+template <typename T, bool IN = false>
 __device__ __forceinline__ C2<T> seg_rhs(const SegCol<T> &c, int iz, int L, bool top_solved, T idz, C2<T> hx, C2<T> hy,
                                          C2<T> hzl, C2<T> hzu, C2<T> hz0)
 {
     const C2<T> sxy = mk<T>(c.kx * hx.x + c.ky * hy.x, c.kx * hx.y + c.ky * hy.y);
     C2<T> dh = csub(hzu, hzl);
-    if (iz == 1) dh = cadd(dh, hz0);
+    if (!IN && iz == 1) dh = cadd(dh, hz0);
     C2<T> r = mk<T>(-sxy.y + dh.x * idz, sxy.x + dh.y * idz);
-    if (c.m00) r = (iz == 1) ? mk<T>(0, 0) : hzl;
-    if (iz == L && !top_solved) r = mk<T>(0, 0);
+    if (c.m00) r = (!IN && iz == 1) ? mk<T>(0, 0) : hzl;
+    if (!IN && iz == L && !top_solved) r = mk<T>(0, 0);
     return r;
 }
 
 // Forward sweep of rows s..s+ns-1 with x_{s-1} left unknown (x_i = y'_i + v'_i x_{s-1} -
 // c'_i x_{i+1}), then the segment's two boundary rows in terms of x_{s-1} and x_{e+1},
 // stored for the reduced solve.  Bands of 109:4-63 (the Neumann top row :33-38, npz >= 2).
-template <typename T, int NSEG>
+// IN: a full segment of interior rows, whose bands are the same on every row.
+template <typename T, int NSEG, bool IN = false>
 __device__ __forceinline__ void seg_eliminate(const SegCol<T> &c, C2<T> (&y)[kRegLev], T (&cp)[kRegLev],
-                                              T (&vp)[kRegLev], int s, int ns, int L, bool top_solved, T idz,
+                                              T (&vp)[kRegLev], int s, int ns_, int L, bool top_solved, T idz,
                                               T idz2, SegShared<T, NSEG> &sh, int k, int lane)
 {
+    const int ns = IN ? kRegLev : ns_;
     T cprev = 0, vprev = 1;
     C2<T> yprev = mk<T>(0, 0);
+    // interior bands: the (0,0) mode's dz-weighted difference rows, else the k^2 rows
+    const T am_in = c.m00 ? -idz : idz2, bm_in = c.m00 ? idz : -(c.k2 + (T)2 * idz2), cm_in = c.m00 ? (T)0 : idz2;
 #pragma unroll
     for (int i = 0; i < kRegLev; ++i) {
         if (i < ns) {
             const int iz = s + i;
             T am, bm, cm;
-            if (iz == L && !top_solved) {
+            if (IN) {
+                am = am_in; bm = bm_in; cm = cm_in;
+            } else if (iz == L && !top_solved) {
                 am = 0; bm = 1; cm = 0;
             } else if (!c.m00) {
                 const bool top = iz == L;
@@ -240,12 +247,13 @@ template <typename T, int NSEG> __device__ __forceinline__ void seg_reduced(SegS
 // Back-substitution of rows s..s+ns-1 from the neighbours' solved boundary values xl =
 // x_{s-1}, xr = x_{e+1}; stores p_hat and the dpdz spectrum, and on segment 0 the Neumann
 // ghost level below the wall (:313-315).
-template <typename T>
+template <typename T, bool IN = false>
 __device__ __forceinline__ void seg_backsub(const C2<T> (&y)[kRegLev], const T (&cp)[kRegLev], const T (&vp)[kRegLev],
-                                            C2<T> xl, C2<T> xr, int s, int ns, int k, int L, C2<T> *ph, C2<T> *dph,
+                                            C2<T> xl, C2<T> xr, int s, int ns_, int k, int L, C2<T> *ph, C2<T> *dph,
                                             long long S, T dz, T rdz, C2<T> hz0)
 {
     using C = C2<T>;
+    const int ns = IN ? kRegLev : ns_;
     // checked build: the segment's rows lie in 1..L
     if (OBL_CHECK && !(ck_in(s - 1, L, CK_TDMA_STORE) && ck_in(s + ns - 1, L + 1, CK_TDMA_STORE))) return;
     C x = mk<T>(0, 0);
@@ -303,6 +311,7 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
     const long long q = c.q;
     const int s = 1 + k * Ls;                                   // first row of the segment
     const int ns = k < K ? min(Ls, L - s + 1) : 0;              // its rows (0: idle warp)
+    const bool interior = ns == kRegLev && s > 1 && s + kRegLev - 1 < L;   // warp-uniform
     C *ph = a.phat + q;
     C *dph = a.dph ? a.dph + q : nullptr;
     if (c.nyq) seg_nyquist<T>(ph, dph, S, s, ns, k, L);
@@ -339,10 +348,18 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
             C hz[kRegLev + 1];
 #pragma unroll
             for (int i = 0; i <= kRegLev; ++i) hz[i] = __ldcs(a.Hz + q + S * min(s + i, L + 1));
+            if (interior) {
 #pragma unroll
-            for (int i = 0; i < kRegLev; ++i) y[i] = seg_rhs<T>(c, s + i, L, top_solved, idz, hx[i], hy[i], hz[i], hz[i + 1], hz0);
+                for (int i = 0; i < kRegLev; ++i)
+                    y[i] = seg_rhs<T, true>(c, s + i, L, top_solved, idz, hx[i], hy[i], hz[i], hz[i + 1], hz0);
+            } else {
+#pragma unroll
+                for (int i = 0; i < kRegLev; ++i)
+                    y[i] = seg_rhs<T>(c, s + i, L, top_solved, idz, hx[i], hy[i], hz[i], hz[i + 1], hz0);
+            }
         }
-        seg_eliminate<T, NSEG>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
+        if (interior) seg_eliminate<T, NSEG, true>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
+        else seg_eliminate<T, NSEG>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
     }
     __syncthreads();
     if (k == 0 && c.act) seg_reduced<T, NSEG>(sh, K, lane);
@@ -350,7 +367,8 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_reg(TdmaA
     if (!c.act || ns == 0) return;
     const C xl = k > 0 ? sh.Ye[k - 1][lane] : mk<T>(0, 0);
     const C xr = k < K - 1 ? sh.Ys[k + 1][lane] : mk<T>(0, 0);
-    seg_backsub<T>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, (T)(1.0 / a.dz), hz0);
+    if (interior) seg_backsub<T, true>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, (T)(1.0 / a.dz), hz0);
+    else seg_backsub<T>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, (T)(1.0 / a.dz), hz0);
 }
 
 bool tdma_reg_supported(int L) { return L >= 1 && L <= kRegSegMax * kRegLev; }
@@ -446,6 +464,7 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_staged(Td
     const long long nunits = nbi + (S + 31) / 32;
     const int s = 1 + k * Ls;
     const int ns = k < K ? min(Ls, L - s + 1) : 0;
+    const bool interior = ns == kRegLev && s > 1 && s + kRegLev - 1 < L;   // warp-uniform
     C *buf = reinterpret_cast<C *>(smraw) + (size_t)k * kStageRows * 32;
     const unsigned bar = smem_addr(&sBar[k]);
     const T dz = (T)a.dz, idz = (T)(1.0 / a.dz), idz2 = (T)(1.0 / (a.dz * a.dz)), rdz = idz;
@@ -524,7 +543,13 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_staged(Td
                     atomicExch(ctl + 1, 1);
                     sAbort = 1;
                 }
-                if (c.act) {
+                if (c.act && interior) {
+#pragma unroll
+                    for (int i = 0; i < kRegLev; ++i)
+                        y[i] = seg_rhs<T, true>(c, s + i, L, top_solved, idz, buf[i * 32 + lane],
+                                                buf[(kRegLev + i) * 32 + lane], buf[(2 * kRegLev + i) * 32 + lane],
+                                                buf[(2 * kRegLev + i + 1) * 32 + lane], hz0);
+                } else if (c.act) {
 #pragma unroll
                     for (int i = 0; i < kRegLev; ++i)
                         y[i] = seg_rhs<T>(c, s + i, L, top_solved, idz, buf[i * 32 + lane], buf[(kRegLev + i) * 32 + lane],
@@ -535,7 +560,8 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_staged(Td
                     pending = true;
                 }
                 if (c.nyq) seg_nyquist<T>(ph, dph, S, s, ns, k, L);
-                if (c.act) seg_eliminate<T, NSEG>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
+                if (c.act && interior) seg_eliminate<T, NSEG, true>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
+                else if (c.act) seg_eliminate<T, NSEG>(c, y, cp, vp, s, ns, L, top_solved, idz, idz2, sh, k, lane);
             }
             __syncthreads();
             if (k == 0 && c.act) seg_reduced<T, NSEG>(sh, K, lane);
@@ -543,7 +569,8 @@ __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_staged(Td
             const C xl = k > 0 ? sh.Ye[k - 1][lane] : mk<T>(0, 0);
             const C xr = k < K - 1 ? sh.Ys[k + 1][lane] : mk<T>(0, 0);
             __syncthreads();   // the next unit's boundary rows overwrite sh
-            if (c.act && ns > 0) seg_backsub<T>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, rdz, hz0);
+            if (c.act && interior) seg_backsub<T, true>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, rdz, hz0);
+            else if (c.act && ns > 0) seg_backsub<T>(y, cp, vp, xl, xr, s, ns, k, L, ph, dph, S, dz, rdz, hz0);
         }
         cur = nxt;
         nxt = sUnit[it & 1];
