@@ -2434,11 +2434,14 @@ extern "C" int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void 
 //   OBL_ENS_SEQUENTIAL  one instance after the other on the ensemble's stream;
 //   OBL_ENS_CONCURRENT  every instance on its own stream, forked from and joined back
 //                       to the ensemble's stream;
-//   OBL_ENS_PERSISTENT  one cooperative launch of the persistent kernel over the work
-//                       list of all instances (ensemble.cuh);
-//   OBL_ENS_PERSISTENT_SPLIT  the same work list in three cooperative launches, one per
+//   OBL_ENS_PERSISTENT  one cooperative launch of the dataflow persistent kernel over the
+//                       work list of all instances (ensemble.cuh: units from one counter,
+//                       each waiting only for its own instance's previous phase);
+//   OBL_ENS_PERSISTENT_SPLIT  the work list in three cooperative launches, one per
 //                       register class (rows | columns + solve | x-inverse), so that the
-//                       light phases run at a higher occupancy.
+//                       light phases run at a higher occupancy;
+//   OBL_ENS_PERSISTENT_BARRIER  one cooperative launch, fixed shares of every phase per
+//                       CTA, phases separated by grid barriers.
 // Any mode can be captured once into a CUDA graph and replayed.
 struct obl_ensemble {
     int dev = 0;
@@ -2451,7 +2454,7 @@ struct obl_ensemble {
     int bps = 0;                          // persistent CTAs per SM (0: all that fit)
     bool phase_stamps = false;            // record the phase boundaries of the persistent kernel
     // persistent mode
-    DevBuf xpad, inst, start, bar;
+    DevBuf xpad, inst, start, bar, flow;
     std::vector<long long> xoff;          // element offset of each instance's 4 x-padded planes
     std::vector<obl_step_io> ios;         // the buffers the uploaded work list was built for
     size_t smem[3] = {0, 0, 0};           // per launch of the persistent step
@@ -2492,19 +2495,25 @@ int ens_ctx_fail(obl_ensemble *ens, int i, int rc)
 struct EnsPart {
     int pb, pe, minb;
 };
-static const EnsPart kEnsAll[1] = {{0, 6, 2}};
+static const EnsPart kEnsAll[1] = {{0, 6, OBL_ENS_MINB}};
 static const EnsPart kEnsSplit[3] = {{0, 1, 2}, {1, 4, 4}, {4, 6, 2}};
 
-template <typename T> static int ens_part_bps(const EnsPart &p, size_t smem)
+static bool ens_persistent(int mode)
 {
+    return mode == OBL_ENS_PERSISTENT || mode == OBL_ENS_PERSISTENT_SPLIT || mode == OBL_ENS_PERSISTENT_BARRIER;
+}
+template <typename T> static int ens_part_bps(const EnsPart &p, size_t smem, bool flow)
+{
+    if (flow) return EnsFlowKernel<T, OBL_ENS_MINB>::blocks_per_sm(smem);
     if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, OBL_ENS_MINB>::blocks_per_sm(smem);
     if (p.pb == 0) return EnsKernel<T, 0, 1, 2>::blocks_per_sm(smem);
     if (p.pb == 1) return EnsKernel<T, 1, 4, 4>::blocks_per_sm(smem);
     return EnsKernel<T, 4, 6, 2>::blocks_per_sm(smem);
 }
 template <typename T> static cudaError_t ens_part_launch(const EnsPart &p, const EnsArgs<T> &a, int blocks, size_t smem,
-                                                        cudaStream_t s)
+                                                        cudaStream_t s, bool flow)
 {
+    if (flow) return EnsFlowKernel<T, OBL_ENS_MINB>::launch(a, blocks, smem, s);
     if (p.pb == 0 && p.pe == 6) return EnsKernel<T, 0, 6, OBL_ENS_MINB>::launch(a, blocks, smem, s);
     if (p.pb == 0) return EnsKernel<T, 0, 1, 2>::launch(a, blocks, smem, s);
     if (p.pb == 1) return EnsKernel<T, 1, 4, 4>::launch(a, blocks, smem, s);
@@ -2529,6 +2538,8 @@ template <typename T> int ens_prepare(obl_ensemble *ens, const obl_step_io *ios)
         for (int i = 0; i < n; ++i) st[(size_t)p * (n + 1) + i + 1] = st[(size_t)p * (n + 1) + i] + h[i].count[p];
     if ((rc = ensure(ens->ctx[0], ens->inst, sizeof(EnsInst<T>) * (size_t)n))) return ens_ctx_fail(ens, 0, rc);
     if ((rc = ensure(ens->ctx[0], ens->start, sizeof(long long) * st.size()))) return ens_ctx_fail(ens, 0, rc);
+    if ((rc = ensure(ens->ctx[0], ens->flow, sizeof(unsigned) * (1 + (size_t)n * kEnsPhases))))
+        return ens_ctx_fail(ens, 0, rc);
     ECK(cudaMemcpyAsync(ens->inst.p, h.data(), sizeof(EnsInst<T>) * (size_t)n, cudaMemcpyHostToDevice, ens->stream));
     ECK(cudaMemcpyAsync(ens->start.p, st.data(), sizeof(long long) * st.size(), cudaMemcpyHostToDevice, ens->stream));
     ECK(cudaStreamSynchronize(ens->stream));
@@ -2540,7 +2551,7 @@ template <typename T> int ens_prepare(obl_ensemble *ens, const obl_step_io *ios)
         size_t smem = 0;
         for (int i = 0; i < n; ++i)
             smem = std::max(smem, EnsGeoHost<T>::smem(ens->ctx[i]->nxt, ens->ctx[i]->nyt, parts[k].pb, parts[k].pe));
-        int per = ens_part_bps<T>(parts[k], smem);
+        int per = ens_part_bps<T>(parts[k], smem, ens->mode == OBL_ENS_PERSISTENT);
         if (per <= 0) return efail(ens, OBL_ERR_UNSUPPORTED, "persistent ensemble kernel cannot be resident");
         if (ens->bps > 0 && ens->bps < per) per = ens->bps;
         ens->smem[k] = smem;
@@ -2555,16 +2566,19 @@ template <typename T> int ens_step_t(obl_ensemble *ens, const obl_step_io *ios)
 {
     const int n = (int)ens->ctx.size();
     int rc;
-    if (ens->mode == OBL_ENS_PERSISTENT || ens->mode == OBL_ENS_PERSISTENT_SPLIT) {
+    if (ens_persistent(ens->mode)) {
         if ((rc = ens_prepare<T>(ens, ios))) return rc;
+        const bool flow = ens->mode == OBL_ENS_PERSISTENT;
         EnsArgs<T> a{(const EnsInst<T> *)ens->inst.p, n, (const long long *)ens->start.p, (unsigned *)ens->bar.p,
                      (int *)((unsigned *)ens->bar.p + 2),
-                     ens->phase_stamps ? (unsigned long long *)((unsigned *)ens->bar.p + 4) : nullptr};
+                     ens->phase_stamps && !flow ? (unsigned long long *)((unsigned *)ens->bar.p + 4) : nullptr,
+                     (unsigned *)ens->flow.p};
         const bool split = ens->mode == OBL_ENS_PERSISTENT_SPLIT;
         for (int k = 0; k < (split ? 3 : 1); ++k) {
-            ECK(cudaMemsetAsync(ens->bar.p, 0, 2 * sizeof(unsigned), ens->stream));
+            if (flow) ECK(cudaMemsetAsync(ens->flow.p, 0, sizeof(unsigned) * (1 + (size_t)n * kEnsPhases), ens->stream));
+            else ECK(cudaMemsetAsync(ens->bar.p, 0, 2 * sizeof(unsigned), ens->stream));
             LaunchScope ls(ens->ctx[0]->rec, "ensemble_persistent", ens->stream);
-            ECK(ens_part_launch<T>((split ? kEnsSplit : kEnsAll)[k], a, ens->nblk[k], ens->smem[k], ens->stream));
+            ECK(ens_part_launch<T>((split ? kEnsSplit : kEnsAll)[k], a, ens->nblk[k], ens->smem[k], ens->stream, flow));
         }
         return OBL_OK;
     }
@@ -2671,6 +2685,7 @@ int obl_ensemble_destroy(obl_ensemble *ens)
     cudaFree(ens->inst.p);
     cudaFree(ens->start.p);
     cudaFree(ens->bar.p);
+    cudaFree(ens->flow.p);
     if (ens->stream) cudaStreamDestroy(ens->stream);
     delete ens;
     return OBL_OK;
@@ -2687,8 +2702,8 @@ int obl_ensemble_context(obl_ensemble *ens, int i, obl_ctx **ctx)
 
 int obl_ensemble_set_mode(obl_ensemble *ens, int mode, int blocks_per_sm)
 {
-    if (!ens || mode < 0 || mode > 3 || blocks_per_sm < 0) return OBL_ERR_ARG;
-    if (mode == OBL_ENS_PERSISTENT || mode == OBL_ENS_PERSISTENT_SPLIT)
+    if (!ens || mode < 0 || mode > OBL_ENS_PERSISTENT_BARRIER || blocks_per_sm < 0) return OBL_ERR_ARG;
+    if (ens_persistent(mode))
         for (auto c : ens->ctx)
             if (!ens_length_supported(c->nxt) || !ens_length_supported(c->nyt))
                 return efail(ens, OBL_ERR_UNSUPPORTED, "persistent ensemble: line length " +

@@ -53,6 +53,9 @@ template <typename T> struct EnsArgs {
     unsigned *bar;                   // [0] arrivals, [1] generation
     int *err;                        // 1: a barrier wait gave up
     unsigned long long *stamps;      // optional: global-timer ns at the start and after each phase
+    // dataflow form: [0] the work counter, [1 + k*kEnsPhases + ph] units of instance k's
+    // phase ph completed (zeroed before each launch)
+    unsigned *flow;
 };
 
 // host-side geometry of the instance kernels (per line length n; 0 if unsupported)
@@ -77,6 +80,18 @@ template <typename T> int ens_wb();   // lines per CTA of the line-minor column 
 template <typename T, int PB, int PE, int MINB> struct EnsKernel {
     static cudaError_t attr(size_t smem);
     static int blocks_per_sm(size_t smem);            // CTAs of the kernel resident per SM
+    static cudaError_t launch(const EnsArgs<T> &a, int blocks, size_t smem, cudaStream_t s);   // cooperative
+};
+
+// The dataflow form of the one-launch persistent kernel (OBL_ENS_PERSISTENT): no grid
+// barriers.  CTAs take units one at a time from a work counter over the whole step's
+// work list (phase-major, instances in order within a phase); a unit of phase ph of
+// instance k first waits until all of that instance's phase ph-1 units have completed
+// (bounded, like the barrier), so instances overlap at phase boundaries instead of the
+// whole grid waiting for the slowest unit of each phase.
+template <typename T, int MINB> struct EnsFlowKernel {
+    static cudaError_t attr(size_t smem);
+    static int blocks_per_sm(size_t smem);
     static cudaError_t launch(const EnsArgs<T> &a, int blocks, size_t smem, cudaStream_t s);   // cooperative
 };
 

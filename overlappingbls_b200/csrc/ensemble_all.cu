@@ -4,4 +4,6 @@
 namespace obl {
 template struct EnsKernel<float, 0, 6, OBL_ENS_MINB>;
 template struct EnsKernel<double, 0, 6, OBL_ENS_MINB>;
+template struct EnsFlowKernel<float, OBL_ENS_MINB>;
+template struct EnsFlowKernel<double, OBL_ENS_MINB>;
 } // namespace obl

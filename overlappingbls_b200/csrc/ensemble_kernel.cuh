@@ -225,6 +225,108 @@ __global__ void __launch_bounds__(256, MINB) k_ensemble(EnsArgs<T> e)
     }
 }
 
+// Bounded wait of thread 0 until *cnt reaches need (another CTA's release: __threadfence
+// then atomicAdd); false once any CTA gave up (err), after raising err itself on timeout.
+__device__ __forceinline__ bool ens_wait_count(const unsigned *cnt, unsigned need, int *err)
+{
+    volatile const unsigned *c = cnt;
+    long long spins = 0;
+    while (*c < need) {
+        if (*(volatile int *)err) return false;
+        if (++spins > kEnsSpinLimit) {
+            atomicExch(err, 1);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    __threadfence();
+    return true;
+}
+
+template <typename T, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_ensemble_flow(EnsArgs<T> e)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C2<T> *sm = reinterpret_cast<C2<T> *>(smraw);
+    __shared__ long long sUnit;
+    __shared__ int sOk;
+    int lk = -1, ln = -1;   // kind and line length of the tables now in shared memory
+    long long total = 0;
+    for (int ph = 0; ph < kEnsPhases; ++ph) total += e.start[(long long)ph * (e.ninst + 1) + e.ninst];
+    for (;;) {
+        __syncthreads();   // the previous unit's reads of sUnit and sOk are done
+        if (threadIdx.x == 0) sUnit = atomicAdd(e.flow, 1u);
+        __syncthreads();
+        long long g = sUnit;
+        if (g >= total) return;
+        // phase and instance of the unit (phase-major list)
+        int ph = 0;
+        const long long *st = e.start;
+        while (g >= st[e.ninst]) {
+            g -= st[e.ninst];
+            ++ph;
+            st += e.ninst + 1;
+        }
+        int k = 0;
+        while (g >= st[k + 1]) ++k;
+        const EnsInst<T> &I = e.inst[k];
+        unsigned *done = e.flow + 1 + (long long)k * kEnsPhases;
+        if (threadIdx.x == 0) sOk = ph == 0 ? 1 : ens_wait_count(done + ph - 1, (unsigned)I.count[ph - 1], e.err);
+        __syncthreads();
+        if (!sOk) return;
+        ens_unit<T>(ph, I, g - st[k], sm, lk, ln);
+        __syncthreads();   // every thread's writes of the unit are issued
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(done + ph, 1u);
+        }
+    }
+}
+
+template <typename T, int MINB> cudaError_t EnsFlowKernel<T, MINB>::attr(size_t smem)
+{
+    static size_t sets[kMaxDevices] = {};
+    const int ds = device_slot();
+    if (ds >= 0 && smem <= sets[ds]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_ensemble_flow<T, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && ds >= 0) sets[ds] = smem;
+    return e;
+}
+
+template <typename T, int MINB> int EnsFlowKernel<T, MINB>::blocks_per_sm(size_t smem)
+{
+    if (attr(smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ensemble_flow<T, MINB>, 256, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per;
+}
+
+template <typename T, int MINB>
+cudaError_t EnsFlowKernel<T, MINB>::launch(const EnsArgs<T> &a, int blocks, size_t smem, cudaStream_t s)
+{
+    cudaError_t e = attr(smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k_ensemble_flow<T, MINB>, a);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
 template <typename T, int PB, int PE, int MINB> cudaError_t EnsKernel<T, PB, PE, MINB>::attr(size_t smem)
 {
     static size_t sets[kMaxDevices] = {};

@@ -101,7 +101,7 @@ def test_ensemble_modes_match_single_instance(prec):
         ctx.synchronize()
         ref.append(b.outputs())
         ctx.close()
-    for mode in ("sequential", "concurrent", "persistent", "persistent_split"):
+    for mode in ("sequential", "concurrent", "persistent", "persistent_split", "persistent_barrier"):
         for graph in (False, True):
             ens.set_mode(mode)
             for b in bufs:
@@ -139,7 +139,7 @@ def test_config4_ensemble_48():
     ens.synchronize()
     ref = [b.outputs()[:8] for b in bufs]
     report = {}
-    for mode in ("sequential", "concurrent", "persistent", "persistent_split"):
+    for mode in ("sequential", "concurrent", "persistent", "persistent_split", "persistent_barrier"):
         ens.set_mode(mode)
         for graph in (False, True):
             ms = ens.time_dev(ios, use_graph=graph, warmup=3, reps=10)
@@ -155,7 +155,7 @@ def test_config4_ensemble_48():
     worst = max(_compare(b.outputs()[:8], r, 1e-6) for b, r in zip(bufs, ref))
     base = report[("sequential", False)]
     for (mode, graph), ms in report.items():
-        print(f"config4 {mode:10s} graph={int(graph)}: {ms:8.3f} ms/step  "
+        print(f"config4 {mode:18s} graph={int(graph)}: {ms:8.3f} ms/step  "
               f"{npts / ms / 1e3:9.1f} Mpts/s  x{base / ms:5.2f} vs sequential")
     print(f"config4 persistent+graph vs sequential: max rel L2 {worst:.2e}; mode {ens.get_mode()}")
     ens.close()
