@@ -316,17 +316,17 @@ int obl_rollout_grad_dev(obl_ctx *ctx, int nsteps, const void *u0, const void *v
      OBL_ENS_CONCURRENT  every instance on its own stream (fork/join);
      OBL_ENS_PERSISTENT  one cooperative launch over the work list of all instances,
                          dispatching on each unit's line lengths at run time (lengths
-                         32..256; divtz planes must be NULL).  CTAs take units from one
-                         work counter; a unit waits only for the previous phase of its
-                         own instance, so instances overlap at phase boundaries.  A wait
+                         32..256; divtz planes must be NULL); every CTA takes a fixed share
+                         of each phase, phases separated by grid barriers.  A barrier wait
                          that gives up is reported by obl_ensemble_synchronize as
                          OBL_ERR_TIMEOUT.
-     OBL_ENS_PERSISTENT_SPLIT  the work list in three cooperative launches, one per
-                         register class (row passes at 2 CTAs/SM, column passes and the
-                         solve at 4), phases separated by grid barriers.
-     OBL_ENS_PERSISTENT_BARRIER  the work list in one cooperative launch, every CTA taking
-                         a fixed share of each phase and the phases separated by grid
-                         barriers (obl_ensemble_phase_times reports its phases).
+     OBL_ENS_PERSISTENT_SPLIT  the same work list in three cooperative launches, one
+                         per register class (row passes at 2 CTAs/SM, column passes and
+                         the solve at 4).
+     OBL_ENS_PERSISTENT_FLOW  one cooperative launch without grid barriers: CTAs take
+                         units from one work counter and a unit waits (bounded) only for
+                         the previous phase of its own instance.  Phase times are recorded
+                         by the barrier forms only.
    obl_ensemble_capture_dev records one step for the given buffers into a CUDA graph
    (after one uncaptured step that allocates every buffer); obl_ensemble_replay
    launches it.  obl_ensemble_time_dev returns the CUDA-event time per step. */
@@ -334,7 +334,7 @@ int obl_rollout_grad_dev(obl_ctx *ctx, int nsteps, const void *u0, const void *v
 #define OBL_ENS_CONCURRENT 1
 #define OBL_ENS_PERSISTENT 2
 #define OBL_ENS_PERSISTENT_SPLIT 3
-#define OBL_ENS_PERSISTENT_BARRIER 4
+#define OBL_ENS_PERSISTENT_FLOW 4
 typedef struct obl_ensemble obl_ensemble;
 int obl_ensemble_create(const obl_grid *grids, int n, const obl_options *opt, obl_ensemble **out);
 int obl_ensemble_destroy(obl_ensemble *ens);

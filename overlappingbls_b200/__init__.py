@@ -59,7 +59,7 @@ EXPORTS = [
     "obl_ensemble_time_dev", "obl_ensemble_phase_times", "obl_ensemble_last_error",
     "obl_slab_sizes", "obl_slab_begin_dev", "obl_slab_solve_dev", "obl_slab_finish_dev",
 ]
-ENS_MODES = {"sequential": 0, "concurrent": 1, "persistent": 2, "persistent_split": 3, "persistent_barrier": 4}
+ENS_MODES = {"sequential": 0, "concurrent": 1, "persistent": 2, "persistent_split": 3, "persistent_flow": 4}
 
 
 class OblError(RuntimeError):

@@ -2434,14 +2434,14 @@ extern "C" int obl_zero_padding_noalloc_dev(obl_ctx *ctx, const void *var, void 
 //   OBL_ENS_SEQUENTIAL  one instance after the other on the ensemble's stream;
 //   OBL_ENS_CONCURRENT  every instance on its own stream, forked from and joined back
 //                       to the ensemble's stream;
-//   OBL_ENS_PERSISTENT  one cooperative launch of the dataflow persistent kernel over the
-//                       work list of all instances (ensemble.cuh: units from one counter,
-//                       each waiting only for its own instance's previous phase);
-//   OBL_ENS_PERSISTENT_SPLIT  the work list in three cooperative launches, one per
+//   OBL_ENS_PERSISTENT  one cooperative launch of the persistent kernel over the work
+//                       list of all instances (ensemble.cuh), phases separated by grid
+//                       barriers;
+//   OBL_ENS_PERSISTENT_SPLIT  the same work list in three cooperative launches, one per
 //                       register class (rows | columns + solve | x-inverse), so that the
 //                       light phases run at a higher occupancy;
-//   OBL_ENS_PERSISTENT_BARRIER  one cooperative launch, fixed shares of every phase per
-//                       CTA, phases separated by grid barriers.
+//   OBL_ENS_PERSISTENT_FLOW  one cooperative launch of the dataflow form (units from one
+//                       counter, each waiting only for its own instance's previous phase).
 // Any mode can be captured once into a CUDA graph and replayed.
 struct obl_ensemble {
     int dev = 0;
@@ -2500,7 +2500,7 @@ static const EnsPart kEnsSplit[3] = {{0, 1, 2}, {1, 4, 4}, {4, 6, 2}};
 
 static bool ens_persistent(int mode)
 {
-    return mode == OBL_ENS_PERSISTENT || mode == OBL_ENS_PERSISTENT_SPLIT || mode == OBL_ENS_PERSISTENT_BARRIER;
+    return mode == OBL_ENS_PERSISTENT || mode == OBL_ENS_PERSISTENT_SPLIT || mode == OBL_ENS_PERSISTENT_FLOW;
 }
 template <typename T> static int ens_part_bps(const EnsPart &p, size_t smem, bool flow)
 {
@@ -2551,7 +2551,7 @@ template <typename T> int ens_prepare(obl_ensemble *ens, const obl_step_io *ios)
         size_t smem = 0;
         for (int i = 0; i < n; ++i)
             smem = std::max(smem, EnsGeoHost<T>::smem(ens->ctx[i]->nxt, ens->ctx[i]->nyt, parts[k].pb, parts[k].pe));
-        int per = ens_part_bps<T>(parts[k], smem, ens->mode == OBL_ENS_PERSISTENT);
+        int per = ens_part_bps<T>(parts[k], smem, ens->mode == OBL_ENS_PERSISTENT_FLOW);
         if (per <= 0) return efail(ens, OBL_ERR_UNSUPPORTED, "persistent ensemble kernel cannot be resident");
         if (ens->bps > 0 && ens->bps < per) per = ens->bps;
         ens->smem[k] = smem;
@@ -2568,7 +2568,7 @@ template <typename T> int ens_step_t(obl_ensemble *ens, const obl_step_io *ios)
     int rc;
     if (ens_persistent(ens->mode)) {
         if ((rc = ens_prepare<T>(ens, ios))) return rc;
-        const bool flow = ens->mode == OBL_ENS_PERSISTENT;
+        const bool flow = ens->mode == OBL_ENS_PERSISTENT_FLOW;
         EnsArgs<T> a{(const EnsInst<T> *)ens->inst.p, n, (const long long *)ens->start.p, (unsigned *)ens->bar.p,
                      (int *)((unsigned *)ens->bar.p + 2),
                      ens->phase_stamps && !flow ? (unsigned long long *)((unsigned *)ens->bar.p + 4) : nullptr,
@@ -2702,7 +2702,7 @@ int obl_ensemble_context(obl_ensemble *ens, int i, obl_ctx **ctx)
 
 int obl_ensemble_set_mode(obl_ensemble *ens, int mode, int blocks_per_sm)
 {
-    if (!ens || mode < 0 || mode > OBL_ENS_PERSISTENT_BARRIER || blocks_per_sm < 0) return OBL_ERR_ARG;
+    if (!ens || mode < 0 || mode > OBL_ENS_PERSISTENT_FLOW || blocks_per_sm < 0) return OBL_ERR_ARG;
     if (ens_persistent(mode))
         for (auto c : ens->ctx)
             if (!ens_length_supported(c->nxt) || !ens_length_supported(c->nyt))

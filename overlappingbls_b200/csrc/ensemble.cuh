@@ -83,7 +83,7 @@ template <typename T, int PB, int PE, int MINB> struct EnsKernel {
     static cudaError_t launch(const EnsArgs<T> &a, int blocks, size_t smem, cudaStream_t s);   // cooperative
 };
 
-// The dataflow form of the one-launch persistent kernel (OBL_ENS_PERSISTENT): no grid
+// The dataflow form of the one-launch persistent kernel (OBL_ENS_PERSISTENT_FLOW): no grid
 // barriers.  CTAs take units one at a time from a work counter over the whole step's
 // work list (phase-major, instances in order within a phase); a unit of phase ph of
 // instance k first waits until all of that instance's phase ph-1 units have completed

@@ -225,13 +225,19 @@ __global__ void __launch_bounds__(256, MINB) k_ensemble(EnsArgs<T> e)
     }
 }
 
-// Bounded wait of thread 0 until *cnt reaches need (another CTA's release: __threadfence
-// then atomicAdd); false once any CTA gave up (err), after raising err itself on timeout.
+// Bounded wait of thread 0 until *cnt reaches need (the counter is raised by release
+// reductions, read here with acquire loads); false once any CTA gave up (err), after
+// raising err itself on timeout.
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ bool ens_wait_count(const unsigned *cnt, unsigned need, int *err)
 {
-    volatile const unsigned *c = cnt;
     long long spins = 0;
-    while (*c < need) {
+    while (ld_acquire(cnt) < need) {
         if (*(volatile int *)err) return false;
         if (++spins > kEnsSpinLimit) {
             atomicExch(err, 1);
@@ -239,47 +245,75 @@ __device__ __forceinline__ bool ens_wait_count(const unsigned *cnt, unsigned nee
         }
         __nanosleep(64);
     }
-    __threadfence();
     return true;
 }
+
+// instances whose phase prefix sums the dataflow kernel keeps in shared memory (more are
+// searched in global memory)
+constexpr int kEnsFlowSmemInst = 64;
 
 template <typename T, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_ensemble_flow(EnsArgs<T> e)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     C2<T> *sm = reinterpret_cast<C2<T> *>(smraw);
-    __shared__ long long sUnit;
+    __shared__ long long sSt[kEnsPhases * (kEnsFlowSmemInst + 1)];
+    __shared__ long long sUnit[2];   // [it & 1]: the unit after next, taken during unit it
     __shared__ int sOk;
+    // (instance, phase) pairs this CTA has seen complete, so that their later units skip the
+    // check (instances past kEnsFlowSmemInst are always checked)
+    __shared__ unsigned char sDone[kEnsFlowSmemInst * kEnsPhases];
     int lk = -1, ln = -1;   // kind and line length of the tables now in shared memory
+    const int n1 = e.ninst + 1;
+    const bool cached = e.ninst <= kEnsFlowSmemInst;
+    if (cached)
+        for (int i = threadIdx.x; i < kEnsPhases * n1; i += blockDim.x) sSt[i] = e.start[i];
+    for (int i = threadIdx.x; i < kEnsFlowSmemInst * kEnsPhases; i += blockDim.x) sDone[i] = 0;
+    const long long *st0 = cached ? sSt : e.start;
     long long total = 0;
-    for (int ph = 0; ph < kEnsPhases; ++ph) total += e.start[(long long)ph * (e.ninst + 1) + e.ninst];
-    for (;;) {
-        __syncthreads();   // the previous unit's reads of sUnit and sOk are done
-        if (threadIdx.x == 0) sUnit = atomicAdd(e.flow, 1u);
-        __syncthreads();
-        long long g = sUnit;
-        if (g >= total) return;
-        // phase and instance of the unit (phase-major list)
+    for (int ph = 0; ph < kEnsPhases; ++ph) total += e.start[(long long)ph * n1 + e.ninst];
+    if (threadIdx.x == 0) {
+        sUnit[0] = atomicAdd(e.flow, 1u);
+        sUnit[1] = atomicAdd(e.flow, 1u);
+    }
+    __syncthreads();
+    long long cur = sUnit[0], nxt = sUnit[1];
+    __syncthreads();   // read before thread 0 overwrites sUnit[0]
+    for (int it = 0; cur < total; ++it) {
+        // the unit after next is taken while this one runs (read after the unit's last barrier)
+        if (threadIdx.x == 0) sUnit[it & 1] = atomicAdd(e.flow, 1u);
+        // phase (the list is phase-major) and instance (binary search of the phase's prefix sums)
+        long long g = cur;
         int ph = 0;
-        const long long *st = e.start;
+        const long long *st = st0;
         while (g >= st[e.ninst]) {
             g -= st[e.ninst];
             ++ph;
-            st += e.ninst + 1;
+            st += n1;
         }
-        int k = 0;
-        while (g >= st[k + 1]) ++k;
+        int lo = 0, hi = e.ninst - 1;   // the instance k with st[k] <= g < st[k+1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (st[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const int k = lo;
         const EnsInst<T> &I = e.inst[k];
         unsigned *done = e.flow + 1 + (long long)k * kEnsPhases;
-        if (threadIdx.x == 0) sOk = ph == 0 ? 1 : ens_wait_count(done + ph - 1, (unsigned)I.count[ph - 1], e.err);
+        if (threadIdx.x == 0) {
+            const bool known = ph == 0 || (k < kEnsFlowSmemInst && sDone[k * kEnsPhases + ph - 1]);
+            sOk = known ? 1 : ens_wait_count(done + ph - 1, (unsigned)I.count[ph - 1], e.err);
+            if (sOk && ph > 0 && k < kEnsFlowSmemInst) sDone[k * kEnsPhases + ph - 1] = 1;
+        }
         __syncthreads();
         if (!sOk) return;
         ens_unit<T>(ph, I, g - st[k], sm, lk, ln);
-        __syncthreads();   // every thread's writes of the unit are issued
-        if (threadIdx.x == 0) {
-            __threadfence();
-            atomicAdd(done + ph, 1u);
-        }
+        __syncthreads();   // every thread's writes of the unit are issued; sOk is read
+        // release: the unit's writes (ordered before by the CTA barrier) become visible to a
+        // CTA that acquires the count; the reduction does not wait for them
+        if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(done + ph) : "memory");
+        cur = nxt;
+        nxt = sUnit[it & 1];
     }
 }
 

@@ -194,7 +194,7 @@ ENSEMBLE_CANDIDATES = (
     {"mode": "persistent", "graph": True, "bps": 0},
     {"mode": "persistent", "graph": True, "bps": 1},
     {"mode": "persistent_split", "graph": True, "bps": 0},
-    {"mode": "persistent_barrier", "graph": True, "bps": 0},
+    {"mode": "persistent_flow", "graph": True, "bps": 0},
 )
 
 

@@ -101,7 +101,7 @@ def test_ensemble_modes_match_single_instance(prec):
         ctx.synchronize()
         ref.append(b.outputs())
         ctx.close()
-    for mode in ("sequential", "concurrent", "persistent", "persistent_split", "persistent_barrier"):
+    for mode in ("sequential", "concurrent", "persistent", "persistent_split", "persistent_flow"):
         for graph in (False, True):
             ens.set_mode(mode)
             for b in bufs:
@@ -139,7 +139,7 @@ def test_config4_ensemble_48():
     ens.synchronize()
     ref = [b.outputs()[:8] for b in bufs]
     report = {}
-    for mode in ("sequential", "concurrent", "persistent", "persistent_split", "persistent_barrier"):
+    for mode in ("sequential", "concurrent", "persistent", "persistent_split", "persistent_flow"):
         ens.set_mode(mode)
         for graph in (False, True):
             ms = ens.time_dev(ios, use_graph=graph, warmup=3, reps=10)

@@ -42,7 +42,7 @@ def test_candidates():
     assert {"fused": 1, "fwd_cluster_size": 8, "fwd_clusters": 0} in tune.step_candidates(96, 96)
     assert all(c["fused"] != 1 for c in tune.step_candidates(96, 64))
     modes = {c["mode"] for c in tune.ENSEMBLE_CANDIDATES}
-    assert modes == {"sequential", "concurrent", "persistent", "persistent_split", "persistent_barrier"}
+    assert modes == {"sequential", "concurrent", "persistent", "persistent_split", "persistent_flow"}
 
 
 def test_step_candidates_include_solve_schedules():
