@@ -7,8 +7,9 @@ Three kinds of entries:
   its cluster size and cluster count) or 2 (one kernel per reference routine).
 * ``ensemble``: per ensemble signature (the multiset of instance shapes and the
   precision) the ensemble mode (sequential, concurrent streams, one persistent launch,
-  the register-class split of it), whether to replay a CUDA graph, and the persistent
-  kernel's CTAs per SM.
+  the register-class split of it, the dataflow form), whether to replay a CUDA graph, and
+  the persistent kernel's CTAs per SM.  ``python -m overlappingbls_b200.tune ensemble
+  --mode MODE`` times the 48-instance ensemble in one mode.
 * ``build``: per bench workload the compile-time schedule of the kernels: CTA shapes of
   the column FFT kernels (warps and lines per CTA, resident warps per SM), the persistent
   prefetching column form, the y-pad's L2 look-ahead, the scratch padding of the row FFT
@@ -289,10 +290,49 @@ def tune_ensemble(ens, ios, shapes, path=None, warmup=3, reps=10, retune=False):
     return best, ms
 
 
+def ensemble48(mode, steps=10, warmup=3, graph=False, blocks_per_sm=0):
+    """Device time per step of the 48-instance ensemble (16 each at 96x96x64, 128x128x96,
+    192x192x128 levels, FP32-mixed) in one mode: (ms, Mpts/s).  Inputs and outputs are
+    device buffers (torch tensors in the storage type)."""
+    import torch
+    import overlappingbls_b200 as obl
+    from overlappingbls_b200 import fields
+    members = fields.ensemble_members()
+    ens = obl.Ensemble([dict(nxt=m["nxt"], nyt=m["nyt"], nzt=m["nzt"], **fields.DOMAIN) for m in members],
+                       precision="mixed")
+    keep, ios, npts = [], [], 0
+    for c, m in zip(ens.contexts, members):
+        f = fields.make_fields(m["nxt"], m["nyt"], m["nzt"], z0=m["z0"], theta_grad=m["theta_grad"], seed=m["seed"])
+        nf = c.ldx * c.nyt * (c.nz + 1)
+        nd = c.ldx * c.nyt * c.nz
+        nb = c.nxt2 * c.nyt2 * (c.nz + 1)
+        dev = lambda n: torch.empty(n, dtype=torch.float32, device="cuda")
+        inp = [torch.from_numpy(np.asarray(f[k], np.float32).ravel(order="F")).cuda() for k in ("u", "v", "w", "theta")]
+        d, big, p, dp = [dev(nf) for _ in range(8)], [dev(nb) for _ in range(4)], dev(nf), [dev(nd) for _ in range(3)]
+        keep += inp + d + big + [p] + dp
+        P = lambda t: t.data_ptr()
+        ios.append(obl.stepio_dev(*(P(t) for t in inp), [P(t) for t in d], [P(t) for t in big], P(p),
+                                  [P(t) for t in dp]))
+        npts += c.nxt * c.nyt * (c.nzt - 1)
+    torch.cuda.synchronize()
+    ens.set_mode(mode, blocks_per_sm)
+    ms = ens.time_dev(ios, use_graph=graph, warmup=warmup, reps=steps)
+    ens.close()
+    return ms, npts / ms / 1e3
+
+
 def main():
     import argparse
-    ap = argparse.ArgumentParser(description="compile-time schedule sweep of the step's kernels")
+    import overlappingbls_b200 as obl
+    ap = argparse.ArgumentParser(description="compile-time schedule sweep of the step's kernels; "
+                                             "ensemble mode timing")
     sub = ap.add_subparsers(dest="cmd", required=True)
+    e = sub.add_parser("ensemble", help="time the 48-instance ensemble in one mode")
+    e.add_argument("--mode", default="persistent", choices=sorted(obl.ENS_MODES))
+    e.add_argument("--steps", type=int, default=10)
+    e.add_argument("--warmup", type=int, default=3)
+    e.add_argument("--graph", action="store_true")
+    e.add_argument("--bps", type=int, default=0)
     b = sub.add_parser("build-variants", help="compile one library per schedule candidate")
     b.add_argument("--out", required=True)
     b.add_argument("--only", nargs="*")
@@ -304,7 +344,11 @@ def main():
     t.add_argument("--warmup", type=int, default=5)
     t.add_argument("--cache", default=None)
     a = ap.parse_args()
-    if a.cmd == "build-variants":
+    if a.cmd == "ensemble":
+        ms, mpts = ensemble48(a.mode, a.steps, a.warmup, a.graph, a.bps)
+        print(json.dumps({"ensemble": "48 instances", "mode": a.mode, "graph": a.graph, "ms_per_step": round(ms, 4),
+                          "Mpts_per_s": round(mpts, 1)}))
+    elif a.cmd == "build-variants":
         for name, lib in build_variants(a.out, a.only).items():
             print(name, lib)
     else:
