@@ -105,7 +105,19 @@ int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
      "tdma_segments"     segments each (kx,ky) column of the pressure solve is split into
                          and solved at once (0 = chosen by size: more than one only when
                          the columns alone cannot fill the GPU; 1 = one sequential sweep;
-                         up to 16; used in the Neumann-top mode with spectral dpdz) */
+                         up to 16; used in the Neumann-top mode with spectral dpdz)
+     "tdma_reg"          FP32 storage: 1 = the register-segmented whole-column solve
+                         (default), 0 = one sequential sweep per column
+     "tdma_stage"        with "tdma_reg": 1 = its persistent form fed by bulk asynchronous
+                         copies (default; needs lhx*nyt even and 16-byte aligned spectra,
+                         else the load-fed form runs), 0 = the load-fed form
+     "gform"             the pressure RHS in G form: 1 = with FP64 storage (default),
+                         2 = always, 0 = never
+     "fwd_chunk"         the step's forward pass over chunks of this many levels (0 = all)
+     "out_streams"       copy streams of the host-array step's outputs (1 or 2; default 2)
+     "fail_alloc"        n > 0: the n-th device allocation from now fails (tests)
+     "stage_timeout_test" 1: the staged solve's waits expect bytes no copy delivers, so
+                         that they give up and OBL_ERR_TIMEOUT is reported (tests) */
 int obl_set_param(obl_ctx *ctx, const char *name, long long value);
 int obl_get_param(obl_ctx *ctx, const char *name, long long *value);
 
