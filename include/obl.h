@@ -113,6 +113,8 @@ int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
                          else the load-fed form runs), 0 = the load-fed form
      "gform"             the pressure RHS in G form: 1 = with FP64 storage (default),
                          2 = always, 0 = never
+     "pad_tma"           FP32 y-pad (zero_padding, the step): 1 = each CTA's input tile by
+                         tensor-map copies (default), 0 = by loads
      "fwd_chunk"         the step's forward pass over chunks of this many levels (0 = all)
      "out_streams"       copy streams of the host-array step's outputs (1 or 2; default 2)
      "fail_alloc"        n > 0: the n-th device allocation from now fails (tests)

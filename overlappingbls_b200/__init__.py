@@ -449,8 +449,10 @@ class Context:
         self._check(self._lib.obl_zero_padding_dev(self._h, var, var_big, nlev), "zero_padding_dev")
 
     def zero_padding_noalloc_dev(self, var, var_big, nlev):
-        """zero_padding into a static device scratch: the call allocates nothing (for
-        callers that may not allocate, e.g. during CUDA graph capture)."""
+        """zero_padding through a static device scratch, allocating nothing: for callers
+        that cannot allocate device memory when they call (an application whose memory
+        pool owns all device memory after start-up, or a latency-critical path where
+        cudaMalloc may block).  Limits as obl.h states (OBL_NOALLOC_SCRATCH_BYTES)."""
         self._check(self._lib.obl_zero_padding_noalloc_dev(self._h, var, var_big, nlev),
                     "zero_padding_noalloc_dev")
 

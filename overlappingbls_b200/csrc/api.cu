@@ -88,6 +88,7 @@ struct obl_ctx {
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
     long long param_tdma_stage = 1;     // the segmented solve fed by bulk asynchronous copies (1) or by loads (0)
     long long param_stage_timeout_test = 0;   // 1: the staged solve's waits expect bytes that never arrive
+    long long param_pad_tma = 1;        // FP32 y-pad: input tiles by tensor-map copies (1) or by loads (0)
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
     long long param_out_streams = 2;    // host step: device -> host copy streams (1 or 2)
     long long param_fwd_chunk = 0;      // forward pass in chunks of this many levels (0 = whole fields)
@@ -138,7 +139,7 @@ static int device_status(obl_ctx *c)
     if (e != cudaSuccess) return cuda_fail(c, e, "device status");
     if (!flag) return OBL_OK;
     cudaMemset(c->d_ctl + 1, 0, sizeof(int));
-    return fail(c, OBL_ERR_TIMEOUT, "pressure solve: a bounded wait for its staged copies gave up");
+    return fail(c, OBL_ERR_TIMEOUT, "a bounded wait for asynchronous copies (pressure solve or y-pad) gave up");
 }
 #define CK(call)                                                                                   \
     do {                                                                                           \
@@ -260,6 +261,8 @@ template <typename T> struct Ops {
         auto ra = rowargs(var, ctx->ldx, xb, nx2, (long long)ny * nlev, 1.0 / nx, OP_PAD, nx);
         if ((rc = rows(OP_PAD, nx, ra, "pad_rows"))) return rc;
         auto ca = colargs(xb, nx2, (long long)nx2 * ny, big, nx2, (long long)nx2 * ny2, nx2, nlev, 1.0 / ny, OP_PAD, ny);
+        ca.tma = (int)ctx->param_pad_tma;
+        ca.wait_err = ctx->d_ctl + 1;
         return cols(OP_PAD, true, ny, ca, "pad_cols");
     }
     // zero_padding through a caller-independent scratch plane xb (nxt2*nyt*nlev reals)
@@ -782,6 +785,8 @@ template <typename T> struct Ops {
             }
             auto ca = colargs(xb, nx2, (long long)nx2 * ny, (T *)io->big[c] + plb * z0, nx2, plb, nx2, nl,
                               1.0 / ny, OP_PAD, ny);
+            ca.tma = (int)ctx->param_pad_tma;
+            ca.wait_err = ctx->d_ctl + 1;
             if ((rc = cols(OP_PAD, true, ny, ca, "pad_cols"))) return rc;
             if ((rc = ddy((T *)io->d[2 * c + 1] + pl * z0, f[c] + pl * z0, nl))) return rc;
             if (H && !(fwd_gform && c != 1)) {   // G form: H_x and H_z are transformed as G in press()
@@ -1570,6 +1575,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "tdma_reg")) return &ctx->param_tdma_reg;
     if (!std::strcmp(name, "tdma_stage")) return &ctx->param_tdma_stage;
     if (!std::strcmp(name, "stage_timeout_test")) return &ctx->param_stage_timeout_test;
+    if (!std::strcmp(name, "pad_tma")) return &ctx->param_pad_tma;
     if (!std::strcmp(name, "gform")) return &ctx->param_gform;
     if (!std::strcmp(name, "out_streams")) return &ctx->param_out_streams;
     if (!std::strcmp(name, "fwd_chunk")) return &ctx->param_fwd_chunk;

@@ -20,8 +20,11 @@
 // scale is applied after the subtraction; derivatives ignore the constant, padding
 // adds it back.  FP32 FFT errors then scale with the fluctuations, not with the mean.
 #pragma once
+#include <cuda.h>   // CUtensorMap and its enums (the encoder is reached through the runtime)
+#include <cstdint>
 #include <vector>
 
+#include "async.cuh"
 #include "fft2.cuh"
 
 namespace obl {
@@ -57,6 +60,8 @@ template <typename T> struct ColArgs {
     int kmul;                        // INV: 0 none, 1 multiply by i*kx(col), 2 by i*ky(row)
     int pf_ahead;                    // the unit of plane z also prefetches its input lines of
                                      // plane z + pf_ahead into L2 (0 = none)
+    int tma;                         // FP32 y-pad: input tile by tensor-map copies (k_cols2_tma)
+    int *wait_err;                   // set to 1 when such a copy's bounded wait gave up
 };
 
 // ----------------------------------------------------------------------------- configuration
@@ -682,6 +687,9 @@ __device__ __forceinline__ void cols2_unit(const ColArgs<T> &a, int bx, int z, c
                 }
             }
         }
+        // an input tile in shared memory may be the exchange scratch itself: every thread
+        // has its elements before the first pass stores into it
+        if constexpr (SMEM_IN) __syncthreads();
         fft_regs<NI, typename D::PF, LL, true, true>(v, sc, twF, t);
     }
     if constexpr (OP == OP_FWD) {
@@ -839,6 +847,87 @@ __global__ void __launch_bounds__(32 * NW, 2) k_cols2_pipe(ColArgs<T> a, int nbx
 #define OBL_COL_PIPE 0   // FP32 y-pad, ddy and y-transform of long lines: persistent prefetching form
 #endif
 
+// ----------------------------------------------------------------------------- TMA-fed y-pad
+// The FP32 y-pad with its CTA's input tile (NI rows x WB real column pairs of the x-padded
+// plane) brought into shared memory by tensor-map copies: one thread issues
+// cp.async.bulk.tensor loads of boxes of 2*WB floats x box_rows rows (64-byte row segments,
+// landing row after row: element i of line l at tile[i*WB + l], the line-minor layout of
+// the exchange scratch), completing on an mbarrier, and the same thread asks L2 for the
+// tile pf_ahead planes later (cp.async.bulk.prefetch.tensor).  The tile lands in the
+// exchange scratch the CTA already holds, so shared memory per CTA and CTAs per SM stay
+// those of k_cols2.  The tensor map covers this GPU's own x-padded planes; no multicast.
+// The wait is bounded: on timeout wait_err is set (the host reports OBL_ERR_TIMEOUT), the
+// CTA waits once more (bounded) for the copy, and its results are not to be used.
+template <typename T, int N, int OP, bool REAL, int NW, int WB>
+__global__ void __launch_bounds__(32 * NW, col_min_blocks(NW, true, col_warps_sm<OP>()))
+    k_cols2_tma(ColArgs<T> a, const __grid_constant__ CUtensorMap tm, int box_rows)
+{
+    using C = C2<T>;
+    using D = LineDerived<N, OP>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ __align__(8) unsigned long long bar;
+    // tensor copies write 128-byte aligned shared memory (an offset from smraw keeps the
+    // pointer in the shared window for the compiler)
+    C *buf = reinterpret_cast<C *>(smraw + ((128u - (smem_addr(smraw) & 127u)) & 127u));
+    const unsigned sbar = smem_addr(&bar);
+    const int x0 = blockIdx.x * 2 * WB, y0 = blockIdx.y * D::NI;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n\tfence.mbarrier_init.release.cluster;\n\t"
+                     "fence.proxy.async.shared::cta;" ::"r"(sbar)
+                     : "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar),
+                     "r"((unsigned)(sizeof(C) * D::NI * WB))
+                     : "memory");
+        for (int y = 0; y < D::NI; y += box_rows)
+            asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                         "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(buf + (size_t)y * WB)),
+                         "l"(&tm), "r"(x0), "r"(y0 + y), "r"(sbar)
+                         : "memory");
+        if (a.pf_ahead > 0 && (int)blockIdx.y + a.pf_ahead < a.nlev)
+            for (int y = 0; y < D::NI; y += box_rows)
+                asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(&tm), "r"(x0),
+                             "r"(y0 + a.pf_ahead * D::NI + y)
+                             : "memory");
+    }
+    __syncthreads();   // the barrier is initialised before anyone waits on it
+    if (!mbar_wait_bounded(sbar, 0)) {
+        if (a.wait_err) atomicExch(a.wait_err, 1);
+        mbar_wait_bounded(sbar, 0);   // a late copy lands before the tile is reused
+    }
+    cols2_unit<T, N, OP, REAL, NW, WB, NoColEpi, true>(a, blockIdx.x, blockIdx.y, a.twF, a.twB, buf, NoColEpi(), buf);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+typedef CUresult (*TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                         const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                         CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                         CUtensorMapFloatOOBfill);
+inline TensorMapEncodeTiled tensor_map_encoder()
+{
+    static TensorMapEncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (TensorMapEncodeTiled)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// rows per tensor copy: NI itself up to 256 rows (the box limit), else the largest divisor
+// of NI not above 256; 0 = no such split
+constexpr int tma_box_rows(int ni)
+{
+    if (ni <= 256) return ni;
+    for (int b = 256; b >= 8; --b)
+        if (ni % b == 0) return b;
+    return 0;
+}
+
 // ----------------------------------------------------------------------------- launchers
 template <typename T, int N, int OP> inline size_t rows_smem()
 {
@@ -907,6 +996,42 @@ template <typename T, int N, int OP, bool REAL> cudaError_t launch_cols_t(const 
     }
     ColArgs<T> a = a0;
     const int nlines = REAL ? a.ncols / 2 : a.ncols;
+    if constexpr (std::is_same<T, float>::value && OP == OP_PAD && REAL && TWG && tma_box_rows(D::NI) > 0) {
+        // the x-padded planes as a 2-D map: ncols floats wide (pitch src_row), NI*nlev rows
+        const bool fits = a.tma && a.src_plane == a.src_row * (long long)D::NI && (a.src_row * 4) % 16 == 0 &&
+                          ((uintptr_t)a.src % 16) == 0 && tensor_map_encoder() != nullptr;
+        if (fits) {
+            constexpr int BR = tma_box_rows(D::NI);
+            CUtensorMap tm;
+            const cuuint64_t dims[2] = {(cuuint64_t)a.ncols, (cuuint64_t)D::NI * a.nlev};
+            const cuuint64_t strides[1] = {(cuuint64_t)a.src_row * sizeof(T)};
+            const cuuint32_t box[2] = {(cuuint32_t)(2 * WB), (cuuint32_t)BR};
+            const cuuint32_t estr[2] = {1, 1};
+            if (tensor_map_encoder()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(a.src), dims, strides,
+                                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return cudaErrorInvalidValue;
+            static int tres[kMaxDevices] = {};
+            auto tk = k_cols2_tma<T, N, OP, REAL, NW, WB>;
+            const size_t tsm = sm + 128;
+            int tr = ds >= 0 ? tres[ds] : 0;
+            if (!tr) {
+                cudaError_t e = cudaFuncSetAttribute(tk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm);
+                if (e != cudaSuccess) return e;
+                int dev = 0, nsm = 0, per = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tk, 32 * NW, tsm);
+                tr = nsm * (per > 0 ? per : 1);
+                if (ds >= 0) tres[ds] = tr;
+            }
+            dim3 grid((nlines + WB - 1) / WB, a.nlev);
+            if (grid.x < 1 || grid.y < 1) return cudaSuccess;
+            if (OBL_COL_PF) a.pf_ahead = (int)((OBL_COL_PF * (long long)tr + 4LL * grid.x - 1) / (4LL * grid.x));
+            tk<<<grid, 32 * NW, tsm, s>>>(a, tm, BR);
+            return cudaGetLastError();
+        }
+    }
     if constexpr (OBL_COL_PIPE && TWG && OP != OP_INV) {
         static int pres[kMaxDevices] = {};
         auto pk = k_cols2_pipe<T, N, OP, REAL, NW, WB>;

@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "async.cuh"
 #include "common.cuh"
 #include "fft.cuh"
 #include "press.cuh"
@@ -419,34 +420,6 @@ template void launch_tdma_reg<float>(const TdmaArgs<float> &, const IslandArgs &
 // product path) is added to the bytes each wait expects: bytes no copy delivers, so that a
 // test can make the waits run out and check the reported status.
 constexpr int kStageRows = 3 * kRegLev + 1;
-constexpr unsigned long long kStageWaitNs = 1000000000ULL;
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok)
-                 : "r"(bar), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
-// true once the phase of the given parity has completed; false after kStageWaitNs
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > kStageWaitNs) return false;
-    return true;
-}
-
 template <int NSEG>
 __global__ void __launch_bounds__(32 * NSEG, kRegSegMax / NSEG) k_tdma_staged(TdmaArgs<float> a, IslandArgs isl, int nbi, int Ls,
                                                               int K, int *ctl, unsigned extra_tx)

@@ -118,3 +118,32 @@ def test_press_stag_array_and_project(orc, grid, prec, top, npz):
     ru, rv, rw = g.project(f["u"], f["v"], f["w"], rdx, rdy, rdz)
     for a, b in ((u, ru), (v, rv), (w, rw)):
         assert rel_l2(a, b) < TOL[prec]
+
+
+@pytest.mark.parametrize("nx,ny,nzt", [(512, 512, 17), (384, 384, 9), (80, 160, 9), (640, 640, 5), (96, 64, 33)])
+def test_y_pad_by_tensor_copies(nx, ny, nzt):
+    """The FP32 y-pad whose input tiles arrive by tensor-map copies (`pad_tma` = 1) gives the
+    results of the load-fed y-pad: through zero_padding and through the step's padded
+    fields.  Boxes of 256, 192, 160, 128 and 64 rows; at nxt = 80 the last box of a plane
+    row runs past the 120 padded columns and is zero-filled."""
+    f = fields.make_fields(nx, ny, nzt)
+    f = {k: np.asfortranarray(v.astype(np.float32).astype(np.float64)) for k, v in f.items()}
+    ctx = obl.Context(nx, ny, nzt, precision="mixed", **fields.DOMAIN)
+    outs = {}
+    for tma in (1, 0):
+        ctx.set_param("pad_tma", tma)
+        big = ctx.big_field()
+        ctx.zero_padding(f["u"], big)
+        u, v, w = (f[k].copy(order="F") for k in "uvw")
+        d = [ctx.field() for _ in range(8)]
+        bigs = [ctx.big_field() for _ in range(4)]
+        p, dp = ctx.field(), [ctx.dfield() for _ in range(3)]
+        ctx.step(u, v, w, f["theta"], d, bigs, p, dp)
+        ctx.synchronize()
+        outs[tma] = [big] + bigs
+    same = all(np.array_equal(a, b) for a, b in zip(outs[1], outs[0]))
+    print(f"y-pad {nx}x{ny}: tensor-copy and load-fed results bitwise equal: {same}")
+    for a, b in zip(outs[1], outs[0]):
+        assert np.isfinite(a).all()
+        assert rel_l2(a, b) < 1e-6
+    ctx.close()
