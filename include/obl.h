@@ -109,8 +109,13 @@ int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
      "tdma_reg"          FP32 storage: 1 = the register-segmented whole-column solve
                          (default), 0 = one sequential sweep per column
      "tdma_stage"        with "tdma_reg": 1 = its persistent form fed by bulk asynchronous
-                         copies (default; needs lhx*nyt even and 16-byte aligned spectra,
-                         else the load-fed form runs), 0 = the load-fed form
+                         copies (needs lhx*nyt even and 16-byte aligned spectra, else the
+                         load-fed form runs), 0 = the load-fed form, 2 = the copy-fed form
+                         above 128 levels, where it measured faster (default)
+     "isl_segments"      mixed mode, whole-column solves of the Neumann-top step: the FP64
+                         island columns split into this many segments by the
+                         column-segmented FP64 solve (0 = 16, capped at L/8; 1 = each island
+                         column swept by one thread inside the FP32 bulk launch)
      "gform"             the pressure RHS in G form: 1 = with FP64 storage (default),
                          2 = always, 0 = never
      "pad_tma"           FP32 y-pad (zero_padding, the step): 1 = each CTA's input tile by

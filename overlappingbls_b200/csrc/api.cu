@@ -86,9 +86,11 @@ struct obl_ctx {
     long long param_tdma_segments = 0;  // column segments of the pressure solve (0 = by size, 1 = one sweep)
     long long param_fail_alloc = 0;     // > 0: the n-th later device allocation fails (failure-path tests)
     long long param_tdma_reg = 1;       // FP32 columns: register-segmented solve (1) or one sweep (0)
-    long long param_tdma_stage = 1;     // the segmented solve fed by bulk asynchronous copies (1) or by loads (0)
+    long long param_tdma_stage = 2;     // the segmented solve fed by bulk asynchronous copies (1), by loads (0),
+                                        // or (2) by copies above 128 levels (16 segments), where it is faster
     long long param_stage_timeout_test = 0;   // 1: the staged solve's waits expect bytes that never arrive
     long long param_pad_tma = 1;        // FP32 y-pad: input tiles by tensor-map copies (1) or by loads (0)
+    long long param_isl_segments = 0;   // segments of each FP64 island column (0 = 16, capped at L/8; 1 = none)
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
     long long param_out_streams = 2;    // host step: device -> host copy streams (1 or 2)
     long long param_fwd_chunk = 0;      // forward pass in chunks of this many levels (0 = whole fields)
@@ -531,15 +533,42 @@ template <typename T> struct Ops {
             bool done = false;
             if constexpr (std::is_same<T, float>::value) {
                 if (ctx->param_tdma_reg && tdma_reg_supported(L)) {
-                    // FP32 bulk columns by the register-segmented solve, FP64 islands by
-                    // their sequential sweep, in one launch
+                    // FP32 bulk columns by the register-segmented solve; FP64 islands either
+                    // split into segments by the column-segmented FP64 solve (two small
+                    // launches first: one thread sweeping all L levels of an island column
+                    // took longer than the whole bulk), or by their sequential sweep inside
+                    // the bulk launch
                     IslandArgs isl{nullptr, 0, nullptr, nullptr};
-                    if (ctx->n_isl) {
+                    const int ip = isl_parts(ta);
+                    if (ip > 1) {
+                        const int seg = (L + ip - 1) / ip, Pn = (L + seg - 1) / seg;
+                        const size_t ni = (size_t)ctx->n_isl * L;
+                        if ((rc = ensure(ctx, ctx->slab_iy, sizeof(double2) * ni)) ||
+                            (rc = ensure(ctx, ctx->slab_iv, sizeof(double) * ni)) ||
+                            (rc = ensure(ctx, ctx->slab_icp, sizeof(double) * ni)) ||
+                            (rc = ensure(ctx, ctx->seg_iface, sizeof(double) * kSlabIface * (size_t)S * Pn)))
+                            return rc;
+                        SlabArgs<T> sa = slab_args(0, 1);
+                        sa.Hx = Hx; sa.Hy = Hy; sa.Hz = Hz; sa.phat = ph; sa.dph = ta.dph;
+                        sa.v = nullptr; sa.cp = nullptr;   // bulk scratch: the island launches do not touch it
+                        sa.iface = (double *)ctx->seg_iface.p;
+                        sa.iface_all = sa.iface;
+                        {
+                            LaunchScope ls(ctx->rec, "tdma_isl_solve", s());
+                            launch_seg_solve_isl<T>(sa, Pn, seg, s(), e);
+                        }
+                        {
+                            LaunchScope ls(ctx->rec, "tdma_isl_finish", s());
+                            launch_seg_finish_isl<T>(sa, Pn, seg, s(), e);
+                        }
+                        if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_isl");
+                    } else if (ctx->n_isl) {
                         if ((rc = ensure(ctx, ctx->isl_c, sizeof(double) * (size_t)ctx->n_isl * L))) return rc;
                         if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
                         isl = IslandArgs{ctx->d_isl, ctx->n_isl, (double *)ctx->isl_c.p, (double2 *)ctx->isl_d.p};
                     }
-                    if (ctx->param_tdma_stage && tdma_staged_supported(ta)) {
+                    const bool stage = ctx->param_tdma_stage == 1 || (ctx->param_tdma_stage == 2 && L > 128);
+                    if (stage && tdma_staged_supported(ta)) {
                         LaunchScope ls(ctx->rec, "tdma_staged", s());
                         launch_tdma_staged(ta, isl, ctx->d_ctl, ctx->param_stage_timeout_test ? 16u : 0u, s(), e);
                         if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_staged");
@@ -1059,6 +1088,16 @@ template <typename T> struct Ops {
         return P > 1 ? (int)P : 1;
     }
     // the solve's column segments for this context (with the spectral dpdz or without)
+    // Segments of each FP64 island column in the mixed mode's whole-column solves (1 = the
+    // island columns sweep inside the FP32 bulk launch).  The column-segmented solve serves
+    // the Neumann-top step with spectral dpdz and the three-spectra RHS.
+    int isl_parts(const TdmaArgs<T> &ta) const
+    {
+        if (!ctx->n_isl || ta.gform || !ta.dph || ctx->opt.top_bc != OBL_TOP_NEUMANN) return 1;
+        const long long P = ctx->param_isl_segments > 0 ? ctx->param_isl_segments : 16;
+        const long long cap = std::min<long long>(kSlabMaxRanks, ctx->L / 8);
+        return (int)std::max<long long>(1, std::min<long long>(P, cap));
+    }
     int solve_parts(bool dpdz) const
     {
         return (ctx->opt.top_bc == OBL_TOP_NEUMANN && dpdz) ? seg_parts(ctx->sp(), ctx->L) : 1;
@@ -1576,6 +1615,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "tdma_stage")) return &ctx->param_tdma_stage;
     if (!std::strcmp(name, "stage_timeout_test")) return &ctx->param_stage_timeout_test;
     if (!std::strcmp(name, "pad_tma")) return &ctx->param_pad_tma;
+    if (!std::strcmp(name, "isl_segments")) return &ctx->param_isl_segments;
     if (!std::strcmp(name, "gform")) return &ctx->param_gform;
     if (!std::strcmp(name, "out_streams")) return &ctx->param_out_streams;
     if (!std::strcmp(name, "fwd_chunk")) return &ctx->param_fwd_chunk;

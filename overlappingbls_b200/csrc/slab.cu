@@ -411,6 +411,22 @@ template <typename T> void launch_seg_finish(const SlabArgs<T> &a, int P, int se
     k_seg_finish<T><<<dim3((unsigned)(nbi + nbb), (unsigned)P), 128, 0, s>>>(a, nbi, seg);
     e = cudaGetLastError();
 }
+template <typename T> void launch_seg_solve_isl(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    const int nbi = (a.n_isl + 127) / 128;   // island blocks only: every block takes the FP64 branch
+    if (nbi < 1) return;
+    k_seg_solve<T><<<dim3((unsigned)nbi, (unsigned)P), 128, 0, s>>>(a, nbi, seg);
+    e = cudaGetLastError();
+}
+template <typename T> void launch_seg_finish_isl(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e)
+{
+    if (e != cudaSuccess) return;
+    const int nbi = (a.n_isl + 127) / 128;
+    if (nbi < 1) return;
+    k_seg_finish<T><<<dim3((unsigned)nbi, (unsigned)P), 128, 0, s>>>(a, nbi, seg);
+    e = cudaGetLastError();
+}
 template <typename T>
 void launch_project_bc_roles(T *u, T *v, T *w, int ldx, int nyt, int nz, int stress_free, int bottom, int top,
                              cudaStream_t s, cudaError_t &e)
@@ -425,6 +441,8 @@ void launch_project_bc_roles(T *u, T *v, T *w, int ldx, int nyt, int nz, int str
     template void launch_slab_finish<T>(const SlabArgs<T> &, cudaStream_t, cudaError_t &);             \
     template void launch_seg_solve<T>(const SlabArgs<T> &, int, int, cudaStream_t, cudaError_t &);     \
     template void launch_seg_finish<T>(const SlabArgs<T> &, int, int, cudaStream_t, cudaError_t &);    \
+    template void launch_seg_solve_isl<T>(const SlabArgs<T> &, int, int, cudaStream_t, cudaError_t &); \
+    template void launch_seg_finish_isl<T>(const SlabArgs<T> &, int, int, cudaStream_t, cudaError_t &); \
     template void launch_project_bc_roles<T>(T *, T *, T *, int, int, int, int, int, int, cudaStream_t,   \
                                              cudaError_t &);
 OBL_INST(float)

@@ -55,6 +55,11 @@ template <typename T> struct SlabArgs {
 // (kx,ky) columns to fill the GPU with one sequential sweep each.
 template <typename T> void launch_seg_solve(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e);
 template <typename T> void launch_seg_finish(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e);
+// the same two launches over the FP64 island columns alone (the mixed mode's whole-column
+// FP32 solves then leave them out): each island column's FP64 chain is split into P
+// segments instead of one thread sweeping all L levels
+template <typename T> void launch_seg_solve_isl(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e);
+template <typename T> void launch_seg_finish_isl(const SlabArgs<T> &a, int P, int seg, cudaStream_t s, cudaError_t &e);
 
 template <typename T> void launch_slab_solve(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e);
 template <typename T> void launch_slab_finish(const SlabArgs<T> &a, cudaStream_t s, cudaError_t &e);

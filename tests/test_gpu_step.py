@@ -319,3 +319,32 @@ def test_forward_pass_in_level_chunks(orc, chunk):
     (d0, b0, p0, dp0, *uvw0), (d1, b1, p1, dp1, *uvw1) = outs
     for a, b in zip(d1 + b1 + [p1] + dp1 + uvw1, d0 + b0 + [p0] + dp0 + uvw0):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("nx,ny,nzt", [(256, 512, 129), (512, 256, 257), (512, 512, 65)])
+def test_island_columns_in_segments(orc, nx, ny, nzt):
+    """The mixed mode's FP64 island columns split into segments by the column-segmented
+    FP64 solve (the default) give the results of their one-thread sequential sweeps inside
+    the FP32 bulk launch (isl_segments = 1), to FP32 storage rounding, and the oracle's."""
+    f = identical_inputs(fields.make_fields(nx, ny, nzt), "mixed")
+    ctx = obl.Context(nx, ny, nzt, precision="mixed", **fields.DOMAIN)
+    ctx.set_param("tdma_segments", 1)
+    L = ctx.nz - 1
+    outs = {}
+    for parts in (0, 1):
+        ctx.set_param("isl_segments", parts)
+        u, v, w = (f[k].copy(order="F") for k in "uvw")
+        d, big, p, dp = _alloc_step(ctx)
+        ctx.step(u, v, w, f["theta"], d, big, p, dp)
+        outs[parts] = (p[:nx, :, :L + 1], [a[:nx, :, :L] for a in dp], u, v, w)
+    a, b = outs[0], outs[1]
+    assert rel_l2(a[0], b[0]) < 1e-7
+    for x, y in zip(a[1], b[1]):
+        assert rel_l2(x, y) < 1e-7
+    for x, y in zip(a[2:], b[2:]):
+        assert rel_l2(x, y) < 1e-7
+    g = orc.Grid(nx, ny, nzt, **fields.DOMAIN)
+    ref = g.step(f["u"], f["v"], f["w"], f["theta"], npz=2)   # nz even on these grids
+    assert rel_l2(a[0], ref["p"][:nx, :, :L + 1]) < 1e-5
+    assert rel_l2(a[4], ref["w"]) < 1e-5
+    ctx.close()
