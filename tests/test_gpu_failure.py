@@ -108,6 +108,7 @@ def test_staged_solve_wait_gives_up(orc):
     f = fields.make_fields(nx, ny, nzt)
     ctx = obl.Context(nx, ny, nzt, precision="mixed", **fields.DOMAIN)
     ctx.set_param("tdma_segments", 1)   # the whole-column solve (few columns pick the column-segmented one)
+    ctx.set_param("tdma_stage", 1)      # its copy-fed form (by default only above 128 levels)
 
     def step():
         u, v, w = (f[k].copy(order="F") for k in "uvw")
