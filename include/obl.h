@@ -116,6 +116,8 @@ int obl_timing_report(obl_ctx *ctx, char *buf, size_t n);
                          island columns split into this many segments by the
                          column-segmented FP64 solve (0 = 16, capped at L/8; 1 = each island
                          column swept by one thread inside the FP32 bulk launch)
+     "isl_concurrent"    1 = those island launches on a side stream beside the bulk launch
+                         (default 0: measured slower)
      "gform"             the pressure RHS in G form: 1 = with FP64 storage (default),
                          2 = always, 0 = never
      "pad_tma"           FP32 y-pad (zero_padding, the step): 1 = each CTA's input tile by

@@ -91,12 +91,17 @@ struct obl_ctx {
     long long param_stage_timeout_test = 0;   // 1: the staged solve's waits expect bytes that never arrive
     long long param_pad_tma = 1;        // FP32 y-pad: input tiles by tensor-map copies (1) or by loads (0)
     long long param_isl_segments = 0;   // segments of each FP64 island column (0 = 16, capped at L/8; 1 = none)
+    long long param_isl_concurrent = 0; // the island launches on a side stream, beside the bulk launch
+                                        // (measured slower: the persistent bulk launch holds every SM)
     long long param_gform = 1;          // pressure RHS in G form: 1 with FP64 storage, 2 always, 0 never
     long long param_out_streams = 2;    // host step: device -> host copy streams (1 or 2)
     long long param_fwd_chunk = 0;      // forward pass in chunks of this many levels (0 = whole fields)
     // overlapped host step: input and output copy streams, per-field events
     cudaStream_t cin = nullptr, cout = nullptr, cout2 = nullptr;
     cudaEvent_t ev[9] = {};
+    // side stream of the solve's FP64 island launches (forked from and joined to `stream`)
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_ev[2] = {};
     std::vector<DevBuf> stage; // host-variant staging (storage type)
     std::vector<DevBuf> stage64;
 
@@ -539,6 +544,7 @@ template <typename T> struct Ops {
                     // took longer than the whole bulk), or by their sequential sweep inside
                     // the bulk launch
                     IslandArgs isl{nullptr, 0, nullptr, nullptr};
+                    bool join_side = false;   // the island launches ran on the side stream
                     const int ip = isl_parts(ta);
                     if (ip > 1) {
                         const int seg = (L + ip - 1) / ip, Pn = (L + seg - 1) / seg;
@@ -553,15 +559,31 @@ template <typename T> struct Ops {
                         sa.v = nullptr; sa.cp = nullptr;   // bulk scratch: the island launches do not touch it
                         sa.iface = (double *)ctx->seg_iface.p;
                         sa.iface_all = sa.iface;
-                        {
-                            LaunchScope ls(ctx->rec, "tdma_isl_solve", s());
-                            launch_seg_solve_isl<T>(sa, Pn, seg, s(), e);
+                        // on a side stream the island launches can run beside the bulk launch
+                        // (on the SMs they hold when it starts; its units go to the others)
+                        cudaStream_t is = s();
+                        if (ctx->param_isl_concurrent) {
+                            if (!ctx->side) {
+                                CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+                                for (auto &ev : ctx->side_ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+                            }
+                            CK(cudaEventRecord(ctx->side_ev[0], s()));
+                            CK(cudaStreamWaitEvent(ctx->side, ctx->side_ev[0], 0));
+                            is = ctx->side;
                         }
                         {
-                            LaunchScope ls(ctx->rec, "tdma_isl_finish", s());
-                            launch_seg_finish_isl<T>(sa, Pn, seg, s(), e);
+                            LaunchScope ls(ctx->rec, "tdma_isl_solve", is);
+                            launch_seg_solve_isl<T>(sa, Pn, seg, is, e);
+                        }
+                        {
+                            LaunchScope ls(ctx->rec, "tdma_isl_finish", is);
+                            launch_seg_finish_isl<T>(sa, Pn, seg, is, e);
                         }
                         if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_isl");
+                        if (is != s()) {
+                            CK(cudaEventRecord(ctx->side_ev[1], is));
+                            join_side = true;
+                        }
                     } else if (ctx->n_isl) {
                         if ((rc = ensure(ctx, ctx->isl_c, sizeof(double) * (size_t)ctx->n_isl * L))) return rc;
                         if ((rc = ensure(ctx, ctx->isl_d, sizeof(double2) * (size_t)ctx->n_isl * (L + 1)))) return rc;
@@ -577,6 +599,7 @@ template <typename T> struct Ops {
                         launch_tdma_reg<float>(ta, isl, s(), e);
                         if (e != cudaSuccess) return cuda_fail(ctx, e, "tdma_reg");
                     }
+                    if (join_side) CK(cudaStreamWaitEvent(s(), ctx->side_ev[1], 0));
                     done = true;
                 }
             }
@@ -1561,6 +1584,9 @@ int obl_ctx_destroy(obl_ctx *ctx)
     if (ctx->cin) cudaStreamDestroy(ctx->cin);
     if (ctx->cout) cudaStreamDestroy(ctx->cout);
     if (ctx->cout2) cudaStreamDestroy(ctx->cout2);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
+    for (auto e : ctx->side_ev)
+        if (e) cudaEventDestroy(e);
     for (auto e : ctx->ev)
         if (e) cudaEventDestroy(e);
     delete ctx;
@@ -1616,6 +1642,7 @@ static long long *param_slot(obl_ctx *ctx, const char *name)
     if (!std::strcmp(name, "stage_timeout_test")) return &ctx->param_stage_timeout_test;
     if (!std::strcmp(name, "pad_tma")) return &ctx->param_pad_tma;
     if (!std::strcmp(name, "isl_segments")) return &ctx->param_isl_segments;
+    if (!std::strcmp(name, "isl_concurrent")) return &ctx->param_isl_concurrent;
     if (!std::strcmp(name, "gform")) return &ctx->param_gform;
     if (!std::strcmp(name, "out_streams")) return &ctx->param_out_streams;
     if (!std::strcmp(name, "fwd_chunk")) return &ctx->param_fwd_chunk;
