@@ -67,3 +67,14 @@ def test_line_lengths_with_plans(n, ok):
 def test_no_device_fails_loudly():
     with pytest.raises(obl.OblError, match="NODEV"):
         obl.Context(64, 64, 65, 1.0, 1.0, 1.0, 1.0, 0.1)
+
+
+def test_every_run_time_parameter_is_documented():
+    """Each name obl_set_param accepts (its table in csrc/api.cu) is described in the
+    obl_set_param comment of include/obl.h, and the comment names no other."""
+    src = open(os.path.join(ROOT, "overlappingbls_b200", "csrc", "api.cu")).read()
+    accepted = set(re.findall(r'std::strcmp\(name, "(\w+)"\)', src))
+    hdr = open(HEADER).read()
+    block = hdr[hdr.index("/* execution tuning"):hdr.index("int obl_set_param")]
+    documented = set(re.findall(r'^\s*"(\w+)"\s', block.replace("/*", " "), re.M))
+    assert accepted and accepted == documented, (sorted(accepted - documented), sorted(documented - accepted))
